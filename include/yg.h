@@ -1,0 +1,167 @@
+/*
+ * yg.h — C-ABI of the B200 visibility gridder.
+ *
+ * A drop-in GPU back end for yandasoft's IVisGridder path
+ * (askap/gridding/IVisGridder.h:64-140) for the SphFunc, WProject, WStack and
+ * AWProject gridders, plus a W-stacking + W-projection hybrid.  The C++
+ * IVisGridder shim that a yandasoft maintainer adds
+ * unpacks its accessor into a yg_chunk and forwards each virtual call to the
+ * function named beside it below.
+ *
+ * Conventions
+ *   - Every function returns 0 (YG_OK) or a YG_ERR_* code; yg_last_error()
+ *     returns the message of the last failure on the calling thread.  The shim
+ *     rethrows it as askap::AskapError, as ASKAPCHECK would.
+ *   - Cubes are the reference's casacore layout: (nrow, nchan, npol),
+ *     column-major (row fastest).  Complex values are interleaved float pairs.
+ *   - Images are (nx, ny, npol, nchan) column-major float, the unpadded shape.
+ *   - A handle is not thread-safe; use one handle per host thread (clone).
+ *     Each handle owns one CUDA stream and its device memory.
+ *   - Host buffers stay caller-owned.  With on_device = 1 every pointer of a
+ *     chunk (except pointing) is a device pointer on the current device.
+ */
+#ifndef YG_H
+#define YG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  YG_OK = 0,
+  YG_ERR_ARG = 1,
+  YG_ERR_CUDA = 2,
+  YG_ERR_FRAC = 3,
+  YG_ERR_WRANGE = 4,
+  YG_ERR_WEIGHT = 5,
+  YG_ERR_CINDEX = 6,
+  YG_ERR_SUPPORT = 7,
+  YG_ERR_STATE = 8,
+  YG_ERR_UNSUPPORTED = 9,
+  YG_ERR_FREQ = 10,
+  YG_ERR_TIMEOUT = 11,
+  YG_ERR_NOMEM = 12
+};
+
+typedef struct yg_gridder yg_gridder;
+typedef struct yg_plan yg_plan;
+
+/* scimath::Axes as the gridder reads it (TableVisGridder::initialiseCellSize,
+ * getImageCentre, getTangentPoint, FrequencyMapper::setupImage). */
+typedef struct yg_axes {
+  double cell[2];        /* direction-axis increments, radians */
+  double centre[2];      /* image centre (ra, dec), radians */
+  double tangent[2];     /* tangent point (ra, dec), radians */
+  int32_t has_freq;      /* 1 if the image has a FREQUENCY axis */
+  int32_t reserved;
+  double freq_start;     /* Hz of the first image channel */
+  double freq_end;       /* Hz of the last image channel */
+} yg_axes;
+
+/* One accessor chunk (accessors::IConstDataAccessor / IDataAccessor). */
+typedef struct yg_chunk {
+  int64_t nrow;
+  int32_t nchan;
+  int32_t npol;
+  const double* uvw;       /* nrow x 3 rotatedUVW(tangent), metres, row-major */
+  const double* delay;     /* nrow uvwRotationDelay(tangent, centre) or NULL */
+  const double* freq;      /* nchan, Hz */
+  float* vis;              /* complex cube; grid reads it, degrid adds into it */
+  const float* noise;      /* complex cube or NULL (noise 1) */
+  const uint8_t* flag;     /* cube or NULL */
+  const int32_t* feed1;    /* nrow or NULL (AWProject, PSF feed selection) */
+  const double* pointing;  /* HOST nrow x 2 pointingDir1 (ra, dec) or NULL */
+  int32_t on_device;       /* 1: uvw, delay, freq, vis, noise, flag, feed1 are device pointers */
+  int32_t reserved;
+} yg_chunk;
+
+/* Last error message of the calling thread. */
+const char* yg_last_error(void);
+
+/* VisGridderFactory::make (askap/gridding/VisGridderFactory.cc:112-285).
+ * parset: "key = value" lines, keys as in a cimager parset with or without the
+ * "Cimager." prefix ("gridder = WProject", "gridder.WProject.wmax = 5000" ...). */
+int yg_create(const char* parset, yg_gridder** out);
+
+/* IVisGridder::clone (IVisGridder.h:77). */
+int yg_clone(const yg_gridder* g, yg_gridder** out);
+
+void yg_destroy(yg_gridder* g);
+
+/* IVisGridder::initialiseGrid (TableVisGridder.cc:997-1030). */
+int yg_initialise_grid(yg_gridder* g, const yg_axes* axes, int32_t nx, int32_t ny, int32_t npol, int32_t nchan,
+                       int32_t dopsf, int32_t dopcf);
+
+/* IVisGridder::grid (TableVisGridder.cc:908-913 -> generic(acc, false)). */
+int yg_grid(yg_gridder* g, const yg_chunk* chunk);
+
+/* IVisGridder::finaliseGrid (TableVisGridder.cc:1109-1236; WStackVisGridder.cc:216-295). */
+int yg_finalise_grid(yg_gridder* g, float* image, int32_t on_device);
+
+/* IVisGridder::finaliseWeights (TableVisGridder.cc:1255-1284). */
+int yg_finalise_weights(yg_gridder* g, float* weights, int32_t on_device);
+
+/* IVisGridder::initialiseDegrid (TableVisGridder.cc:1286-1319; WStackVisGridder.cc:297-337). */
+int yg_initialise_degrid(yg_gridder* g, const yg_axes* axes, int32_t nx, int32_t ny, int32_t npol, int32_t nchan,
+                         const float* image, int32_t on_device);
+
+/* IVisGridder::degrid (TableVisGridder.cc:898-902 -> generic(acc, true)); adds
+ * the model visibilities into chunk->vis. */
+int yg_degrid(yg_gridder* g, yg_chunk* chunk);
+
+/* IVisGridder::finaliseDegrid (TableVisGridder.cc:1364-1372). */
+int yg_finalise_degrid(yg_gridder* g);
+
+/* IVisGridder::customiseForContext (TableVisGridder.cc:1381-1405). */
+int yg_customise_for_context(yg_gridder* g, const char* context);
+
+/* IVisGridder::initVisWeights with VisWeightsMultiFrequency(reffreq)
+ * (VisGridderFactory.cc:265-272). */
+int yg_init_vis_weights_mfs(yg_gridder* g, double reffreq);
+
+/* IVisGridder::isModelEmpty (TableVisGridder.cc:1466-1469). */
+int yg_is_model_empty(const yg_gridder* g, int32_t* empty);
+
+/* ---- inspection (itsSupport, itsOverSample, itsConvFunc, itsSumWeights) ---- */
+int yg_get_support(const yg_gridder* g, int32_t* support, int32_t* oversample, int32_t* ncf);
+/* CF cache: sizes[ncf] (2S+1), offsets[ncf] (complex elements), data (complex). */
+int yg_get_cf(const yg_gridder* g, int32_t* sizes, int64_t* offsets, float* data, int64_t data_capacity);
+/* itsConvFuncOffsets: 2 ints per plane; *n receives the number of planes. */
+int yg_get_cf_offsets(const yg_gridder* g, int32_t* offsets, int32_t capacity, int32_t* n);
+/* itsSumWeights (rows, npol, nchan) column-major; *nrows receives rows. */
+int yg_get_sum_weights(const yg_gridder* g, double* out, int64_t capacity, int32_t* nrows);
+/* itsGrid: ngrids x (nx, ny, npol, nchan) complex, padded shape. */
+int yg_get_grid(const yg_gridder* g, float* out, int64_t capacity_complex, int32_t* ngrids);
+/* padded grid shape */
+int yg_get_shape(const yg_gridder* g, int32_t* nx, int32_t* ny, int32_t* npol, int32_t* nchan);
+/* stats: samples/taps gridded, samples/taps degridded, ms grid, ms degrid, ms CF, CF planes built */
+int yg_get_stats(const yg_gridder* g, double* out8);
+/* builds the convolution functions for the current axes without data
+ * (SphFunc, WProject, WStack; AWProject builds from data). */
+int yg_build_cf(yg_gridder* g);
+
+/* ---- plans: bin a chunk once, grid/degrid it many times (major cycle) ---- */
+int yg_plan_create(yg_gridder* g, const yg_chunk* chunk, yg_plan** out);
+int yg_plan_grid(yg_gridder* g, const yg_plan* plan, const yg_chunk* chunk);
+int yg_plan_degrid(yg_gridder* g, yg_plan* plan, yg_chunk* chunk);
+/* on-grid samples and work items of a plan */
+int yg_plan_info(const yg_plan* plan, int64_t* nvalid, int32_t* nitems, int32_t* tile);
+/* per sample (row + nrow*chan order): grid position iu, iv (with the CF
+ * offset applied; 0 off-grid), CF index, status (0 unused, 1 w out of range,
+ * 2 off the grid, 3 gridded) */
+int yg_plan_samples(const yg_gridder* g, const yg_plan* plan, int32_t* iu, int32_t* iv, int32_t* cfi,
+                    uint8_t* status);
+void yg_plan_destroy(yg_plan* plan);
+
+/* ---- tuning ---- */
+int yg_set_tile(yg_gridder* g, int32_t tile);      /* 0 = automatic */
+int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
+int yg_synchronize(yg_gridder* g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YG_H */

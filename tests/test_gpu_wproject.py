@@ -1,0 +1,161 @@
+"""WProject on the GPU vs the oracle (the minimum slice of the gridder).
+
+Tolerances: cell/plane/oversample indices bit-exact; grid and visibilities
+within 1e-5 relative L2 of the oracle; CF taps within 1e-5 of each plane's
+peak (FP32 FFTs of different libraries); sums of weights exact."""
+import numpy as np
+import pytest
+
+from parity_helpers import ARCSEC, make_pair, rel_l2, snapped_model
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def wp(ygmod, oracle_mod, c0_small):
+    ds, p = c0_small
+    params = dict(wmax=p["wmax"], nwplanes=p["nwplanes"], oversample=p["oversample"], cutoff=p["cutoff"],
+                  maxsupport=p["maxsupport"])
+    og, gg = make_pair("WProject", params)
+    cell = p["cell_arcsec"] * ARCSEC
+    return ds, p, og, gg, cell
+
+
+def check_finalise(img_gpu, img_cpu, grid, grdsf):
+    """finaliseGrid = grid correction x real(backward FFT).  The correction
+    reaches ~135 at the field edge and amplifies FP32 FFT rounding there, so
+    the transform is compared with the correction divided out (1e-5), and both
+    FP32 images are compared with an FP64 evaluation of the same step: the GPU
+    must be at least as close to it as the FP32 restatement."""
+    from oracle import cf as cfm
+    cx, cy = cfm.sph_correction_vectors(grid.shape, grdsf)
+    corr = (cx[:, None] * cy[None, :])[:, :, None, None]
+    safe = np.where(corr == 0, 1.0, corr)
+    err_raw = rel_l2(img_gpu / safe, img_cpu / safe)
+    assert err_raw < TOL, err_raw
+    g64 = grid.astype(np.complex128)
+    f64 = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(g64, axes=(0, 1)), axes=(0, 1)), axes=(0, 1)).real
+    img64 = f64 * corr * (grid.shape[0] * grid.shape[1])
+    e_gpu, e_cpu = rel_l2(img_gpu, img64), rel_l2(img_cpu, img64)
+    print("finaliseGrid rel error vs FP64: gpu %.3e  fp32 restatement %.3e" % (e_gpu, e_cpu))
+    assert e_gpu <= 2 * e_cpu + 1e-7
+
+
+def _acc(ds, vis=None):
+    from yandasoft_b200.gridder import Accessor
+    return Accessor(ds.uvw, ds.freq, ds.vis if vis is None else vis, noise=ds.noise, flag=ds.flag)
+
+
+def test_indices_bit_exact(wp):
+    import oracle
+    from yandasoft_b200.gridder import Axes
+    ds, p, og, gg, cell = wp
+    nx = p["nx"]
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    gg.build_cf()
+    acc = _acc(ds).to_device()
+    plan = gg.plan(acc)
+    iu, iv, cfi, st = plan.samples(gg, acc)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.init_cf()
+    s_cpu = og.cache.support
+    s_gpu, os_, ncf = gg.support()
+    assert s_gpu == s_cpu
+    oiu, oiv, ofu, ofv = oracle.indices(ds.uvw, ds.freq, og.uvcell[0], og.uvcell[1], og.os, nx, nx)
+    planes = og.ws.plane_map(ds.uvw, ds.freq)
+    ocfi = ofu + og.os * (ofv + og.os * planes)
+    on = (oiu - s_cpu > 0) & (oiv - s_cpu > 0) & (oiu + s_cpu < nx) & (oiv + s_cpu < nx)
+    assert np.array_equal(st == 3, on)
+    assert np.array_equal(st[~on], np.full((~on).sum(), 2, dtype=np.uint8))
+    assert np.array_equal(iu[on], oiu[on])
+    assert np.array_equal(iv[on], oiv[on])
+    assert np.array_equal(cfi[on], ocfi[on])
+
+
+def test_cf_parity(wp):
+    ds, p, og, gg, cell = wp
+    og.init_cf()
+    cpu = og.cache.cfs
+    gpu = gg.convolution_functions()
+    assert len(cpu) == len(gpu)
+    worst = 0.0
+    for a, b in zip(cpu, gpu):
+        assert a.shape == b.shape
+        worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+    assert worst < TOL, worst
+
+
+def test_grid_parity(wp):
+    from yandasoft_b200.gridder import Axes
+    ds, p, og, gg, cell = wp
+    nx = p["nx"]
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    gg.grid(_acc(ds))
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(__import__("oracle").Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag))
+    g_gpu = gg.grids()[0]
+    g_cpu = og.grids[0]
+    err = rel_l2(g_gpu, g_cpu)
+    assert err < TOL, err
+    assert np.array_equal(gg.sum_weights(), og.sumw)
+    # finaliseGrid in isolation: the oracle's FFT + grid correction applied to
+    # the GPU's own grid
+    img_gpu = gg.finaliseGrid()
+    og.grids = [g_gpu.copy()]
+    img_cpu_same_grid = og.finalise_grid()
+    check_finalise(img_gpu, img_cpu_same_grid, g_gpu, og.grdsf)
+
+
+def test_degrid_parity(wp):
+    import oracle
+    from yandasoft_b200.gridder import Axes
+    ds, p, og, gg, cell = wp
+    nx = p["nx"]
+    model, comp = snapped_model(ds, nx, cell)
+    gd = gg.clone()
+    gd.initialiseDegrid(Axes(cell, cell), model)
+    vis_gpu = np.zeros_like(ds.vis)
+    gd.degrid(_acc(ds, vis_gpu))
+    og.initialise_degrid(model, cell, cell)
+    vis_cpu = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vis_cpu, noise=ds.noise, flag=ds.flag))
+    err = rel_l2(vis_gpu, vis_cpu)
+    assert err < TOL, err
+    # error of both against the FP64 measurement equation (reported, loose bound)
+    ref = oracle.dft(ds.uvw, ds.freq, comp)
+    iu, iv, _, _ = oracle.indices(ds.uvw, ds.freq, og.uvcell[0], og.uvcell[1], og.os, nx, nx)
+    s = og.cache.support
+    on = (iu - s > 0) & (iv - s > 0) & (iu + s < nx) & (iv + s < nx)
+    e_gpu = rel_l2(vis_gpu[:, :, 0][on], ref[on])
+    e_cpu = rel_l2(vis_cpu[:, :, 0][on], ref[on])
+    print("degrid rel error vs FP64 DFT: gpu %.3e cpu %.3e" % (e_gpu, e_cpu))
+    assert abs(e_gpu - e_cpu) < 1e-4
+
+
+def test_grid_linearity_and_plan_reuse(wp):
+    """grid(a v1 + b v2) = a grid(v1) + b grid(v2); a plan reused for two passes
+    gives twice one pass."""
+    from yandasoft_b200.gridder import Accessor, Axes
+    ds, p, og, gg, cell = wp
+    nx = p["nx"]
+    g1 = gg.clone()
+    g1.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    acc = _acc(ds).to_device()
+    plan = g1.plan(acc)
+    g1.grid_plan(plan, acc)
+    once = g1.grids()[0].copy()
+    g1.grid_plan(plan, acc)
+    twice = g1.grids()[0]
+    assert rel_l2(twice, 2 * once) < TOL
+    rng = np.random.default_rng(5)
+    v2 = np.asfortranarray((rng.standard_normal(ds.vis.shape) + 1j * rng.standard_normal(ds.vis.shape)).astype(np.complex64))
+    a, b = 0.75, -1.5
+    res = []
+    for v in (ds.vis, v2, np.asfortranarray((a * ds.vis + b * v2).astype(np.complex64))):
+        gx = gg.clone()
+        gx.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+        gx.grid(Accessor(ds.uvw, ds.freq, v, noise=ds.noise, flag=ds.flag))
+        res.append(gx.grids()[0])
+    assert rel_l2(res[2], a * res[0] + b * res[1]) < 1e-5

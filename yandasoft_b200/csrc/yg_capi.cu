@@ -1,0 +1,345 @@
+// extern "C" boundary of the B200 gridder: translates between the plain C
+// structures of include/yg.h and the C++ Gridder, and turns exceptions into
+// status codes plus a thread-local message (the reference's ASKAPCHECK /
+// AskapError convention, askap/gridding/*.cc).
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/yg.h"
+#include "yg_gridder.h"
+
+struct yg_gridder {
+  std::unique_ptr<yg::Gridder> g;
+};
+
+struct yg_plan {
+  yg::Plan pl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return YG_OK;
+  } catch (const yg::YgError& e) {
+    return fail(e.code, e.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(YG_ERR_NOMEM, "out of host memory");
+  } catch (const std::exception& e) {
+    return fail(YG_ERR_ARG, e.what());
+  } catch (...) {
+    return fail(YG_ERR_ARG, "unknown error");
+  }
+}
+
+yg::Axes to_axes(const yg_axes* a) {
+  yg::Axes x;
+  if (!a) throw yg::YgError{YG_ERR_ARG, "axes must not be NULL"};
+  x.cell[0] = a->cell[0];
+  x.cell[1] = a->cell[1];
+  x.centre[0] = a->centre[0];
+  x.centre[1] = a->centre[1];
+  x.tangent[0] = a->tangent[0];
+  x.tangent[1] = a->tangent[1];
+  x.has_freq = a->has_freq;
+  x.freq_start = a->freq_start;
+  x.freq_end = a->freq_end;
+  return x;
+}
+
+yg::Chunk to_chunk(const yg_chunk* c) {
+  if (!c) throw yg::YgError{YG_ERR_ARG, "chunk must not be NULL"};
+  if (c->nrow < 0 || c->nchan < 0 || c->npol <= 0) throw yg::YgError{YG_ERR_ARG, "bad chunk shape"};
+  if (c->nrow > 0 && c->nchan > 0 && (!c->uvw || !c->freq || !c->vis))
+    throw yg::YgError{YG_ERR_ARG, "chunk needs uvw, freq and vis"};
+  yg::Chunk x;
+  x.nrow = c->nrow;
+  x.nchan = c->nchan;
+  x.npol = c->npol;
+  x.uvw = c->uvw;
+  x.delay = c->delay;
+  x.freq = c->freq;
+  x.vis = reinterpret_cast<float2*>(c->vis);
+  x.noise = reinterpret_cast<const float2*>(c->noise);
+  x.flag = c->flag;
+  x.feed1 = c->feed1;
+  x.pointing = c->pointing;
+  x.on_device = c->on_device;
+  return x;
+}
+
+yg::Gridder& G(yg_gridder* g) {
+  if (!g || !g->g) throw yg::YgError{YG_ERR_ARG, "NULL gridder handle"};
+  return *g->g;
+}
+
+const yg::Gridder& G(const yg_gridder* g) {
+  if (!g || !g->g) throw yg::YgError{YG_ERR_ARG, "NULL gridder handle"};
+  return *g->g;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* yg_last_error(void) { return g_last_error.c_str(); }
+
+int yg_create(const char* parset, yg_gridder** out) {
+  return guarded([&] {
+    if (!parset || !out) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    *out = nullptr;
+    auto h = std::make_unique<yg_gridder>();
+    h->g = yg::Gridder::make(yg::Parset::parse(parset));
+    *out = h.release();
+  });
+}
+
+int yg_clone(const yg_gridder* g, yg_gridder** out) {
+  return guarded([&] {
+    if (!out) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    auto h = std::make_unique<yg_gridder>();
+    h->g = G(g).clone();
+    *out = h.release();
+  });
+}
+
+void yg_destroy(yg_gridder* g) { delete g; }
+
+int yg_initialise_grid(yg_gridder* g, const yg_axes* axes, int32_t nx, int32_t ny, int32_t npol, int32_t nchan,
+                       int32_t dopsf, int32_t dopcf) {
+  return guarded([&] { G(g).initialise_grid(to_axes(axes), nx, ny, npol, nchan, dopsf != 0, dopcf != 0); });
+}
+
+int yg_grid(yg_gridder* g, const yg_chunk* chunk) {
+  return guarded([&] { G(g).grid(to_chunk(chunk)); });
+}
+
+int yg_finalise_grid(yg_gridder* g, float* image, int32_t on_device) {
+  return guarded([&] {
+    if (!image) throw yg::YgError{YG_ERR_ARG, "NULL image"};
+    G(g).finalise_grid(image, on_device != 0);
+  });
+}
+
+int yg_finalise_weights(yg_gridder* g, float* weights, int32_t on_device) {
+  return guarded([&] {
+    if (!weights) throw yg::YgError{YG_ERR_ARG, "NULL weights"};
+    G(g).finalise_weights(weights, on_device != 0);
+  });
+}
+
+int yg_initialise_degrid(yg_gridder* g, const yg_axes* axes, int32_t nx, int32_t ny, int32_t npol, int32_t nchan,
+                         const float* image, int32_t on_device) {
+  return guarded([&] {
+    if (!image) throw yg::YgError{YG_ERR_ARG, "NULL image"};
+    G(g).initialise_degrid(to_axes(axes), nx, ny, npol, nchan, image, on_device != 0);
+  });
+}
+
+int yg_degrid(yg_gridder* g, yg_chunk* chunk) {
+  return guarded([&] {
+    yg::Chunk c = to_chunk(chunk);
+    G(g).degrid(c);
+  });
+}
+
+int yg_finalise_degrid(yg_gridder* g) {
+  return guarded([&] { G(g).finalise_degrid(); });
+}
+
+int yg_customise_for_context(yg_gridder* g, const char* context) {
+  return guarded([&] { G(g).customise_for_context(context ? context : ""); });
+}
+
+int yg_init_vis_weights_mfs(yg_gridder* g, double reffreq) {
+  return guarded([&] { G(g).init_vis_weights_mfs(reffreq); });
+}
+
+int yg_is_model_empty(const yg_gridder* g, int32_t* empty) {
+  return guarded([&] {
+    if (!empty) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    *empty = G(g).is_model_empty() ? 1 : 0;
+  });
+}
+
+int yg_get_support(const yg_gridder* g, int32_t* support, int32_t* oversample, int32_t* ncf) {
+  return guarded([&] {
+    const yg::Gridder& x = G(g);
+    if (support) *support = x.support();
+    if (oversample) *oversample = x.oversample();
+    if (ncf) *ncf = x.ncf();
+  });
+}
+
+int yg_get_cf(const yg_gridder* g, int32_t* sizes, int64_t* offsets, float* data, int64_t data_capacity) {
+  return guarded([&] {
+    const yg::Gridder& x = G(g);
+    std::vector<int> s;
+    std::vector<long long> o;
+    x.cf_sizes(s, o);
+    if (sizes) std::memcpy(sizes, s.data(), s.size() * sizeof(int));
+    if (offsets)
+      for (size_t i = 0; i < o.size(); ++i) offsets[i] = o[i];
+    if (data) {
+      std::vector<float2> d;
+      x.cf_data(d);
+      if ((int64_t)d.size() > data_capacity) throw yg::YgError{YG_ERR_ARG, "CF buffer too small"};
+      std::memcpy(data, d.data(), d.size() * sizeof(float2));
+    }
+  });
+}
+
+int yg_get_cf_offsets(const yg_gridder* g, int32_t* offsets, int32_t capacity, int32_t* n) {
+  return guarded([&] {
+    std::vector<int2> o;
+    G(g).cf_offsets(o);
+    if (n) *n = (int32_t)o.size();
+    if (offsets) {
+      if ((int32_t)o.size() > capacity) throw yg::YgError{YG_ERR_ARG, "offset buffer too small"};
+      for (size_t i = 0; i < o.size(); ++i) {
+        offsets[2 * i] = o[i].x;
+        offsets[2 * i + 1] = o[i].y;
+      }
+    }
+  });
+}
+
+int yg_get_sum_weights(const yg_gridder* g, double* out, int64_t capacity, int32_t* nrows) {
+  return guarded([&] {
+    std::vector<double> w;
+    int rows = 0;
+    G(g).sum_weights(w, &rows);
+    if (nrows) *nrows = rows;
+    if (out) {
+      if ((int64_t)w.size() > capacity) throw yg::YgError{YG_ERR_ARG, "buffer too small"};
+      std::memcpy(out, w.data(), w.size() * sizeof(double));
+    }
+  });
+}
+
+int yg_get_grid(const yg_gridder* g, float* out, int64_t capacity_complex, int32_t* ngrids) {
+  return guarded([&] {
+    const yg::Gridder& x = G(g);
+    if (ngrids) *ngrids = x.ngrids();
+    if (out) {
+      std::vector<float2> d;
+      x.grid_data(d);
+      if ((int64_t)d.size() > capacity_complex) throw yg::YgError{YG_ERR_ARG, "grid buffer too small"};
+      std::memcpy(out, d.data(), d.size() * sizeof(float2));
+    }
+  });
+}
+
+int yg_get_shape(const yg_gridder* g, int32_t* nx, int32_t* ny, int32_t* npol, int32_t* nchan) {
+  return guarded([&] {
+    int a, b, c, d;
+    G(g).shape(&a, &b, &c, &d);
+    if (nx) *nx = a;
+    if (ny) *ny = b;
+    if (npol) *npol = c;
+    if (nchan) *nchan = d;
+  });
+}
+
+int yg_get_stats(const yg_gridder* g, double* out8) {
+  return guarded([&] {
+    if (!out8) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    const yg::Stats& s = G(g).stats();
+    out8[0] = s.samples_gridded;
+    out8[1] = s.taps_gridded;
+    out8[2] = s.samples_degridded;
+    out8[3] = s.taps_degridded;
+    out8[4] = s.time_grid_ms;
+    out8[5] = s.time_degrid_ms;
+    out8[6] = s.time_cf_ms;
+    out8[7] = s.cf_generations;
+  });
+}
+
+int yg_build_cf(yg_gridder* g) {
+  return guarded([&] { G(g).build_cf(); });
+}
+
+int yg_plan_create(yg_gridder* g, const yg_chunk* chunk, yg_plan** out) {
+  return guarded([&] {
+    if (!out) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    yg::Gridder& x = G(g);
+    yg::Chunk c = to_chunk(chunk);
+    if (!c.on_device) throw yg::YgError{YG_ERR_ARG, "plans need device-resident chunks"};
+    auto p = std::make_unique<yg_plan>();
+    x.prepare_plan_cf(c);
+    x.bin(c, p->pl);
+    *out = p.release();
+  });
+}
+
+int yg_plan_grid(yg_gridder* g, const yg_plan* plan, const yg_chunk* chunk) {
+  return guarded([&] {
+    if (!plan) throw yg::YgError{YG_ERR_ARG, "NULL plan"};
+    yg::Chunk c = to_chunk(chunk);
+    if (!c.on_device) throw yg::YgError{YG_ERR_ARG, "plans need device-resident chunks"};
+    G(g).grid_plan(c, plan->pl);
+  });
+}
+
+int yg_plan_degrid(yg_gridder* g, yg_plan* plan, yg_chunk* chunk) {
+  return guarded([&] {
+    if (!plan) throw yg::YgError{YG_ERR_ARG, "NULL plan"};
+    yg::Chunk c = to_chunk(chunk);
+    if (!c.on_device) throw yg::YgError{YG_ERR_ARG, "plans need device-resident chunks"};
+    yg::Gridder& x = G(g);
+    if (x.is_model_empty()) return;
+    x.degrid_plan(c, plan->pl);
+  });
+}
+
+int yg_plan_info(const yg_plan* plan, int64_t* nvalid, int32_t* nitems, int32_t* tile) {
+  return guarded([&] {
+    if (!plan) throw yg::YgError{YG_ERR_ARG, "NULL plan"};
+    if (nvalid) *nvalid = plan->pl.nvalid;
+    if (nitems) *nitems = plan->pl.nitems;
+    if (tile) *tile = plan->pl.tile;
+  });
+}
+
+int yg_plan_samples(const yg_gridder* g, const yg_plan* plan, int32_t* iu, int32_t* iv, int32_t* cfi,
+                    uint8_t* status) {
+  return guarded([&] {
+    if (!plan || !iu || !iv || !cfi || !status) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    G(g).plan_samples(plan->pl, iu, iv, cfi, status);
+  });
+}
+
+void yg_plan_destroy(yg_plan* plan) { delete plan; }
+
+int yg_set_tile(yg_gridder* g, int32_t tile) {
+  return guarded([&] {
+    if (tile < 0 || (tile > 0 && tile < 8)) throw yg::YgError{YG_ERR_ARG, "tile must be 0 or >= 8"};
+    G(g).set_tile(tile);
+  });
+}
+
+int yg_set_item_size(yg_gridder* g, int32_t vmax) {
+  return guarded([&] {
+    if (vmax < 1) throw yg::YgError{YG_ERR_ARG, "item size must be positive"};
+    G(g).set_vmax(vmax);
+  });
+}
+
+int yg_synchronize(yg_gridder* g) {
+  return guarded([&] { G(g).sync(); });
+}
+
+}  // extern "C"

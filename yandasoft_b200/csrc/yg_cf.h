@@ -1,0 +1,71 @@
+// Convolution-function cache and its GPU builders.
+#pragma once
+#include <vector>
+
+#include "yg_internal.h"
+
+namespace yg {
+
+struct CFCacheDev {
+  DevBuf data, off, size, offsets;
+  int ncf = 0;
+  int noffsets = 0;
+  int maxsize = 0;
+  int support = 0;          // itsSupport
+  long long total = 0;      // complex elements
+  std::vector<int> h_size;
+  std::vector<long long> h_off;
+  std::vector<int2> h_offsets;
+  CFView view() const;
+  int layout(const std::vector<int>& sizes, const std::vector<int2>& offs);
+  int download(std::vector<float2>& out) const;
+};
+
+struct WProjCFParams {
+  int shape_x = 0, shape_y = 0;   // padded grid shape
+  double uvcell_u = 0, uvcell_v = 0;
+  int os = 8;
+  int maxsupport = 256;
+  std::vector<double> wterms;     // per w-plane (wavelengths)
+  double cutoff = 1e-3;
+  bool cutoff_abs = false;
+  int limitsupport = 0;
+  bool variablesupport = false;
+  bool offsetsupport = false;
+  double alpha = 1.0;
+};
+
+struct AWCFParams : WProjCFParams {
+  double diameter = 12.0;
+  double blockage = 2.0;
+  int maxfeeds = 1;
+  int maxfields = 1;
+  int nchan_cf = 1;               // channels of the cache (1 unless frequency dependent)
+  std::vector<double> freqs;      // per cache channel
+};
+
+struct AWFeedJob {
+  int feed;
+  int field;
+  double l, m;                    // beam offset direction cosines (0 for the PSF)
+};
+
+int cf_build_sphfunc(CFCacheDev& cache, int support, int os, double alpha);
+int cf_build_wproject(CFCacheDev& cache, const WProjCFParams& p, DevBuf& work, cudaStream_t st);
+int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeedJob>& jobs, DevBuf& work,
+                cudaStream_t st);
+
+// gridding entry points (yg_gridding.cu)
+int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st);
+int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
+              DevBuf& scratch, DevError* err, cudaStream_t st);
+int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
+              int nchan_img, double* sumw, DevError* err, cudaStream_t st);
+int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
+                int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
+                cudaStream_t st);
+int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
+size_t grid_smem_bytes(int npol, int P);
+int grid_pols_per_pass(int npol, int P);
+
+}  // namespace yg

@@ -1,0 +1,198 @@
+// C++ host side of the B200 gridder: the IVisGridder surface
+// (askap/gridding/IVisGridder.h:64-140) and the VisGridderFactory parset
+// handling (askap/gridding/VisGridderFactory.cc:112-285) for the SphFunc,
+// WProject, WStack and AWProject gridders, on top of the CUDA kernels.
+#pragma once
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "yg_cf.h"
+#include "yg_image.h"
+#include "yg_internal.h"
+#include "yg_spheroidal.h"
+
+namespace yg {
+
+class Parset {
+ public:
+  static Parset parse(const std::string& text);
+  bool has(const std::string& k) const { return kv_.count(k) > 0; }
+  std::string get(const std::string& k, const std::string& dflt) const;
+  std::string get(const std::string& k) const;  // throws when missing
+  double get_double(const std::string& k, double dflt) const;
+  int get_int(const std::string& k, int dflt) const;
+  bool get_bool(const std::string& k, bool dflt) const;
+  Parset subset(const std::string& prefix) const;
+  std::map<std::string, std::string> kv_;
+};
+
+struct YgError {
+  int code;
+  std::string msg;
+};
+
+// image axes: what initialiseCellSize / FrequencyMapper / getImageCentre read
+struct Axes {
+  double cell[2] = {0, 0};        // direction axis increments (radians)
+  double centre[2] = {0, 0};      // image centre (ra, dec) radians
+  double tangent[2] = {0, 0};     // tangent point (ra, dec) radians
+  int has_freq = 0;
+  double freq_start = 0, freq_end = 0;
+};
+
+// one accessor chunk
+struct Chunk {
+  long long nrow = 0;
+  int nchan = 0, npol = 0;
+  const double* uvw = nullptr;
+  const double* delay = nullptr;
+  const double* freq = nullptr;
+  float2* vis = nullptr;
+  const float2* noise = nullptr;
+  const uint8_t* flag = nullptr;
+  const int* feed1 = nullptr;
+  const double* pointing = nullptr;
+  int on_device = 0;
+};
+
+enum class Kind { SphFunc, WProject, WStack, AWProject, WStackWProject };
+
+struct Stats {
+  double samples_gridded = 0, taps_gridded = 0;
+  double samples_degridded = 0, taps_degridded = 0;
+  double time_grid_ms = 0, time_degrid_ms = 0, time_cf_ms = 0;
+  double cf_generations = 0;
+};
+
+class Gridder {
+ public:
+  // VisGridderFactory::make
+  static std::unique_ptr<Gridder> make(const Parset& parset);
+  std::unique_ptr<Gridder> clone() const;
+  ~Gridder();
+
+  void initialise_grid(const Axes& axes, int nx, int ny, int npol, int nchan, bool dopsf, bool dopcf);
+  void grid(const Chunk& c);
+  void finalise_grid(float* out, bool out_on_device);
+  void finalise_weights(float* out, bool out_on_device);
+  void initialise_degrid(const Axes& axes, int nx, int ny, int npol, int nchan, const float* image, bool on_device);
+  void degrid(Chunk& c);
+  void finalise_degrid();
+  void customise_for_context(const std::string& context);
+  void init_vis_weights_mfs(double reffreq);
+  bool is_model_empty() const { return model_empty_; }
+
+  // inspection helpers
+  Kind kind() const { return kind_; }
+  int support() const { return cf_.support; }
+  int oversample() const { return os_; }
+  int ncf() const { return cf_.ncf; }
+  void cf_sizes(std::vector<int>& sizes, std::vector<long long>& offs) const { sizes = cf_.h_size; offs = cf_.h_off; }
+  void cf_offsets(std::vector<int2>& o) const { o = cf_.h_offsets; }
+  void cf_data(std::vector<float2>& out) const;
+  void sum_weights(std::vector<double>& out, int* nrows) const;
+  void grid_data(std::vector<float2>& out) const;
+  long long grid_elems() const;
+  int ngrids() const;
+  const Stats& stats() const { return stats_; }
+  void shape(int* nx, int* ny, int* npol, int* nchan) const;
+  double uvcell(int i) const { return uvcell_[i]; }
+  // explicit CF build without data (WProject/SphFunc/WStack)
+  void build_cf();
+  float2* device_grid() { return grids_.as<float2>(); }
+  cudaStream_t stream() const { return stream_; }
+  // plan-level API for repeated passes over the same data
+  void bin(const Chunk& c, Plan& pl);
+  void grid_plan(const Chunk& c, const Plan& pl);
+  void degrid_plan(Chunk& c, Plan& pl);
+  void set_tile(int t) { tile_override_ = t; }
+  int tile_for(int smax, int npol) const;
+  int items_vmax() const { return vmax_; }
+  void set_vmax(int v) { vmax_ = v; }
+  void sync();
+  void ensure_device();
+  // builds whatever CFs a chunk needs (AWProject builds from the data)
+  void prepare_plan_cf(const Chunk& c) {
+    ensure_device();
+    init_cf(c);
+  }
+  // per-sample on-grid position (with CF offset), CF index and status of a plan
+  void plan_samples(const Plan& pl, int* iu, int* iv, int* cfi, unsigned char* status) const;
+
+ private:
+  Gridder() = default;
+  void configure(Kind k, const Parset& sub, const Parset& full);
+  void init_axes(const Axes& axes, int nx, int ny, int npol, int nchan);
+  void init_sumw();
+  void init_cf(const Chunk& dc);
+  void check_error();
+  void upload_chunk(const Chunk& c, Chunk& dc, bool need_vis, bool vis_writable);
+  std::vector<int> chan_map(const double* freq_host, int nchan) const;
+  void fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, const uint8_t* row_ok) const;
+  double wterm_cf(int plane) const;
+  void prepare_corrections();
+  std::vector<uint8_t> psf_rows(const Chunk& hc);
+
+  Kind kind_ = Kind::SphFunc;
+  // parameters
+  int os_ = 128;
+  int sph_support_ = 3;
+  double alpha_ = 1.0;
+  WSampling ws_{};           // CF-side w sampling (W gridders)
+  WSampling ws_stack_{};     // stack sampling (WStackWProject)
+  double wmax_ = 0;
+  double cutoff_ = 1e-3;
+  bool cutoff_abs_ = false;
+  int maxsupport_ = 256;
+  int limitsupport_ = 0;
+  bool variablesupport_ = false;
+  bool offsetsupport_ = false;
+  bool track_per_os_ = false;
+  bool alldatapsf_ = false;
+  double max_pointing_sep_ = -1.0;
+  float padding_ = 1.0f;
+  bool clear_grids_ = false;
+  // AW
+  double diameter_ = 12.0, blockage_ = 2.0;
+  int maxfeeds_ = 1, maxfields_ = 1;
+  bool freqdep_ = true;
+  double pointing_tol_ = 1e-4, pa_tol_ = 0.1, freq_tol_ = 1e-6;
+  std::vector<std::vector<int>> aw_done_;          // [field][feed]
+  std::vector<std::vector<std::pair<double, double>>> aw_pointings_;
+  std::vector<double> aw_cached_freqs_;
+  int aw_last_field_ = -1, aw_current_field_ = 0;
+  int aw_nchan_ = 0;
+  // MFS weights
+  bool mfs_ = false;
+  double mfs_reffreq_ = 1.405e9;
+  int mfs_order_ = 0;
+
+  // state
+  Axes axes_;
+  int nx_ = 0, ny_ = 0, npol_ = 0, nchan_ = 0;
+  double uvcell_[2] = {0, 0};
+  bool psf_ = false, pcf_ = false;
+  bool model_empty_ = false;
+  bool first_psf_row_ = true;
+  int rep_feed_ = 0;
+  double rep_pointing_[2] = {0, 0};
+  int tile_override_ = 0;
+  int vmax_ = 1024;
+
+  CFCacheDev cf_;
+  bool cf_built_ = false;
+  DevBuf grids_, sumw_, carry_, err_, chanmap_d_, rowok_d_, corr_d_;
+  DevBuf up_uvw_, up_delay_, up_freq_, up_vis_, up_noise_, up_flag_, up_feed_;
+  DevBuf scratch_, tmpvals_, cfwork_, img_tmp_, mfs_d_;
+  int nsumw_rows_ = 1;
+  Plan plan_;
+  ImageFFT fft_;
+  cudaStream_t stream_ = nullptr;
+  Stats stats_;
+  int device_ = 0;
+  bool device_ready_ = false;
+};
+
+}  // namespace yg

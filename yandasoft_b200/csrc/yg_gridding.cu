@@ -1,0 +1,939 @@
+// Binning, tiled gridding and degridding kernels of the B200 gridder.
+//
+// Pipeline of one grid (or degrid) pass over a chunk of visibilities:
+//   k_bin          one thread per (row, chan) sample: FP64 bit-exact uv cell,
+//                  oversample offsets, w-plane, CF index, strict on-grid test
+//                  (TableVisGridder.cc:604-764), and a 64-bit sort key
+//                  (grid plane, image channel, uv tile, CF index, Morton
+//                  position inside the tile).
+//   radix sort     cub::DeviceRadixSort (library call) of (key, sample id).
+//   k_tile_bounds  start/end of every tile's run in the sorted list.
+//   work items     tiles split into items of at most vmax samples.
+//   k_grid         one CTA per item: the padded tile (T + 2 Smax)^2 lives in
+//                  shared memory; every thread owns the cells of a fixed
+//                  residue class (x mod W, y mod W), W = 2 Smax + 1, so no two
+//                  threads ever touch the same cell and the tap sums run in
+//                  registers until a thread's cell changes (no atomics).  The
+//                  padded tile is flushed once to a per-item scratch slot.
+//   k_halo_sum     each output tile adds, in a fixed order, the overlapping
+//                  parts of its neighbours' padded tiles: deterministic, no
+//                  atomics, and the grid is written once.
+//   k_degrid       one CTA per item: the padded grid tile is staged in shared
+//                  memory, one warp per visibility, warp-shuffle reduction.
+//   k_degrid_writeback  the reference's write-back semantics, including the
+//                  value it carries into off-grid samples.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "yg_internal.h"
+
+namespace yg {
+
+
+__device__ __forceinline__ unsigned int morton2(unsigned int x, unsigned int y) {
+  auto spread = [](unsigned int v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1);
+}
+
+// ---------------------------------------------------------------------------
+// k_bin
+// status: 0 = not used (flagged / unmapped / rejected row), 1 = w out of range
+// (clipped), 2 = valid but off the grid, 3 = gridded/degridded.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(BinArgs a, unsigned long long* __restrict__ key, unsigned int* __restrict__ val,
+                      unsigned int* __restrict__ pos, int* __restrict__ cfi_out,
+                      unsigned char* __restrict__ status, DevError* err) {
+  const long long n = a.nrow * (long long)a.nchan;
+  const long long ntiles = (long long)a.ntx * a.nty;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n;
+       s += (long long)gridDim.x * blockDim.x) {
+    const long long row = s % a.nrow;
+    const int chan = (int)(s / a.nrow);
+    unsigned long long k = a.invalid_key;
+    unsigned int p = 0;
+    int cfi = 0;
+    unsigned char st = 0;
+    if (!a.row_ok || a.row_ok[row]) {
+      const double f = a.freq[chan];
+      const double u = a.uvw[3 * row + 0], v = a.uvw[3 * row + 1], w = a.uvw[3 * row + 2];
+      int iu, iv, fu, fv;
+      if (!axis_index(f, u, a.cellu, a.os, a.nx, &iu, &fu) || !axis_index(f, v, a.cellv, a.os, a.ny, &iv, &fv)) {
+        raise_error(err, YG_ERR_FRAC, s);
+      } else {
+        // w-plane indices are computed for every sample, as initIndices does
+        int e = 0, plane = 0, gind = 0;
+        if (a.cf_mode != CF_MODE_SINGLE || a.grid_mode != GRID_MODE_SINGLE) {
+          const double wf = __dmul_rn(__ddiv_rn(w, kC), f);
+          if (a.cf_mode == CF_MODE_WSTACK_WPROJ) {
+            gind = get_wplane(a.ws_stack, wf, &e);
+            if (gind >= 0) {
+              const int half = (a.ws_stack.nwplanes - 1) / 2;
+              const double wst = __dmul_rn((double)(gind - half), a.ws_stack.wscale);
+              plane = get_wplane(a.ws, __dsub_rn(wf, wst), &e);
+            } else {
+              plane = -1;
+            }
+          } else {
+            plane = get_wplane(a.ws, wf, &e);
+            gind = (a.grid_mode == GRID_MODE_WPLANE) ? plane : 0;
+          }
+          if (e) raise_error(err, e, s);
+        }
+        int cplane = 0;
+        if (a.cf_mode == CF_MODE_WPLANE || a.cf_mode == CF_MODE_WSTACK_WPROJ) {
+          cplane = plane;
+        } else if (a.cf_mode == CF_MODE_AW) {
+          const int fd = a.feed ? a.feed[row] : 0;
+          cplane = plane;
+          if (plane >= 0) {
+            const int c = a.aw_nchan > 1 ? chan : 0;
+            cplane = plane + a.ws.nwplanes * (c + a.aw_nchan * (fd + a.aw_maxfeeds * a.aw_field));
+          }
+        }
+        bool good = true;
+        if (a.flag) {
+          for (int pol = 0; pol < a.npol; ++pol) {
+            if (a.flag[s + n * pol]) { good = false; break; }
+          }
+        }
+        const int ichan = a.chan_map[chan];
+        if (good && ichan >= 0) {
+          if (gind < 0 || cplane < 0) {
+            st = 1;
+          } else {
+            cfi = fu + a.os * (fv + a.os * cplane);
+            if (cfi < 0 || cfi >= a.cf.ncf || a.cf.size[cfi] <= 0) {
+              raise_error(err, YG_ERR_CINDEX, s);
+            } else {
+              const int support = (a.cf.size[cfi] - 1) / 2;
+              int offu = 0, offv = 0;
+              if (a.cf.offsets && cplane < a.cf.noffsets) {
+                const int2 o = a.cf.offsets[cplane];
+                offu = o.x;
+                offv = o.y;
+              }
+              const int iuo = iu + offu, ivo = iv + offv;
+              if ((iuo - support) > 0 && (ivo - support) > 0 && (iuo + support) < a.nx && (ivo + support) < a.ny) {
+                st = 3;
+                const int tx = iuo / a.tile, ty = ivo / a.tile;
+                const long long tile = tx + (long long)a.ntx * ty;
+                const long long gc = (long long)gind * a.nchan_img + ichan;
+                const unsigned int m = morton2((unsigned)(iuo - tx * a.tile), (unsigned)(ivo - ty * a.tile));
+                k = (((unsigned long long)(gc * ntiles + tile) * (unsigned long long)a.cf.ncf + (unsigned)cfi)
+                     << a.mbits) | m;
+                p = (unsigned)iuo | ((unsigned)ivo << 16);
+              } else {
+                st = 2;
+              }
+            }
+          }
+        }
+      }
+    }
+    key[s] = k;
+    val[s] = (unsigned int)s;
+    pos[s] = p;
+    cfi_out[s] = cfi;
+    status[s] = st;
+  }
+}
+
+// tile id of a sorted key
+__device__ __forceinline__ long long key_tile(unsigned long long k, int mbits, int ncf) {
+  return (long long)((k >> mbits) / (unsigned long long)ncf);
+}
+
+__global__ void k_tile_bounds(const unsigned long long* __restrict__ key, long long n, int mbits, int ncf,
+                              unsigned long long invalid_key, int* __restrict__ tstart, int* __restrict__ tend,
+                              long long* nvalid) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = key[i];
+    if (k >= invalid_key) continue;
+    const long long t = key_tile(k, mbits, ncf);
+    if (i == 0 || key_tile(key[i - 1], mbits, ncf) != t) tstart[t] = (int)i;
+    const bool last = (i == n - 1) || key[i + 1] >= invalid_key;
+    if (last || key_tile(key[i + 1], mbits, ncf) != t) tend[t] = (int)(i + 1);
+    if (last) *nvalid = i + 1;
+  }
+}
+
+__global__ void k_count_items(const int* __restrict__ tstart, const int* __restrict__ tend, long long ntiles,
+                              int vmax, int* __restrict__ nit) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles; t += (long long)gridDim.x * blockDim.x) {
+    const int c = tend[t] - tstart[t];
+    nit[t] = c > 0 ? (c + vmax - 1) / vmax : 0;
+  }
+}
+
+__global__ void k_fill_items(const int* __restrict__ tstart, const int* __restrict__ tend,
+                             const int* __restrict__ nit, const int* __restrict__ base, long long ntiles, int vmax,
+                             int4* __restrict__ items) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles; t += (long long)gridDim.x * blockDim.x) {
+    const int m = nit[t];
+    const int b = base[t];
+    for (int j = 0; j < m; ++j) {
+      const int s0 = tstart[t] + j * vmax;
+      const int s1 = min(tend[t], s0 + vmax);
+      items[b + j] = make_int4((int)t, s0, s1, 0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weights: rVis = phasor * conj(vis) * wt (* mfs), TableVisGridder.cc:775-806
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float noise_weight(float nre) {
+  const float vn = __fmul_rn(nre, nre);
+  return (vn > 0.f) ? (float)(1.0 / (double)vn) : 0.f;
+}
+
+__device__ __forceinline__ void phasor_of(const VisArgs& v, long long row, int chan, float* pr, float* pi) {
+  if (!v.delay) {
+    *pr = 1.f;
+    *pi = 0.f;
+    return;
+  }
+  const double ph = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(2.0, kPi), v.freq[chan]), v.delay[row]), kC);
+  *pr = (float)cos(ph);
+  *pi = (float)sin(ph);
+}
+
+// sum of weights per (row, pol, image channel), double (TableVisGridder.cc:783-823)
+__global__ void k_sumw(VisArgs v, const unsigned char* __restrict__ status, const int* __restrict__ cfi,
+                       const int* __restrict__ chan_map, int os, int track_per_os, int nrows_sumw, int nchan_img,
+                       double* __restrict__ sumw, DevError* err) {
+  const long long n = v.nrow * (long long)v.nchan;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+    if (status[s] != 3) continue;
+    const long long row = s % v.nrow;
+    if (v.psf && v.psf_ok && !v.psf_ok[row]) continue;
+    const int chan = (int)(s / v.nrow);
+    const int c = cfi[s];
+    const int r = track_per_os ? c : c / (os * os);
+    const int ic = chan_map[chan];
+    if (r < 0 || r >= nrows_sumw || ic < 0 || ic >= nchan_img) { raise_error(err, YG_ERR_CINDEX, s); continue; }
+    for (int p = 0; p < v.npol; ++p) {
+      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
+      const float wt = noise_weight(nre);
+      if (!(wt > 0.f)) { raise_error(err, YG_ERR_WEIGHT, s); continue; }
+      atomicAdd(&sumw[r + (long long)nrows_sumw * (p + (long long)v.npol * ic)], (double)wt);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_grid
+// ---------------------------------------------------------------------------
+struct GridKArgs {
+  const int4* items;
+  const unsigned int* val;   // sample ids, sorted
+  const unsigned int* pos;   // iu | iv << 16, unsorted (by sample id)
+  const int* cfi;            // unsorted
+  VisArgs v;
+  CFView cf;
+  int tile, ntx;
+  long long ntiles;
+  int smax;                  // Smax of the plan
+  int P;                     // T + 2 Smax
+  float2* scratch;           // [item][npol][P][P]
+  int pol0;                  // first polarisation of this pass
+  int npol_total;            // polarisations of the visibility cube
+  DevError* err;
+};
+
+constexpr int kGridThreads = 256;
+constexpr int kBatch = 64;
+
+struct VisRec {
+  int px0, py0;      // footprint origin inside the padded tile
+  int mx, my;        // px0 mod W, py0 mod W
+  int w;             // 2S+1 of this CF
+  int pad_;
+  long long cfoff;   // CF offset (elements)
+};
+
+template <int NPOL, int MAXSLOTS>
+__global__ void __launch_bounds__(kGridThreads) k_grid(GridKArgs a) {
+  extern __shared__ float4 smem_raw[];
+  float2* acc_s = reinterpret_cast<float2*>(smem_raw);
+  const int P = a.P;
+  const int P2 = P * P;
+  VisRec* recs = reinterpret_cast<VisRec*>(acc_s + (size_t)NPOL * P2);
+  float2* vals = reinterpret_cast<float2*>(recs + kBatch);
+
+  const int4 it = a.items[blockIdx.x];
+  const long long tile_id = it.x;
+  const long long t = tile_id % a.ntiles;
+  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
+  const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
+  const int W = 2 * a.smax + 1;
+  const int W2 = W * W;
+
+  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
+
+  int rx[MAXSLOTS], ry[MAXSLOTS], cur[MAXSLOTS];
+  float2 acc[MAXSLOTS][NPOL];
+#pragma unroll
+  for (int q = 0; q < MAXSLOTS; ++q) {
+    const int k = q * blockDim.x + threadIdx.x;
+    rx[q] = k < W2 ? k % W : -1;
+    ry[q] = k < W2 ? k / W : -1;
+    cur[q] = -1;
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) acc[q][p] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+
+  const long long n = a.v.nrow * (long long)a.v.nchan;
+  for (int base = it.y; base < it.z; base += kBatch) {
+    const int nb = min(kBatch, it.z - base);
+    // stage visibility records
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+      const unsigned int s = a.val[base + j];
+      const unsigned int ps = a.pos[s];
+      const int c = a.cfi[s];
+      const int w = a.cf.size[c];
+      const int sup = (w - 1) / 2;
+      VisRec r;
+      r.px0 = (int)(ps & 0xffffu) - sup - X0;
+      r.py0 = (int)(ps >> 16) - sup - Y0;
+      r.mx = r.px0 % W;
+      r.my = r.py0 % W;
+      r.w = w;
+      r.pad_ = 0;
+      r.cfoff = a.cf.off[c];
+      recs[j] = r;
+      const long long row = s % a.v.nrow;
+      const int chan = (int)(s / a.v.nrow);
+      float pr, pi;
+      phasor_of(a.v, row, chan, &pr, &pi);
+      const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+      const bool use = !(a.v.psf && a.v.psf_ok && !a.v.psf_ok[row]);
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        const int pp = a.pol0 + p;
+        const float nre = a.v.noise ? a.v.noise[s + n * pp].x : 1.f;
+        const float wt = noise_weight(nre);
+        float2 o;
+        if (a.v.psf) {
+          o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
+          o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
+        } else {
+          const float2 vv = a.v.vis[s + n * pp];
+          const float vr = vv.x, vi = -vv.y;
+          float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+          float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+          rr = __fmul_rn(__fmul_rn(rr, wt), m);
+          ri = __fmul_rn(__fmul_rn(ri, wt), m);
+          o = make_float2(rr, ri);
+        }
+        if (!use) o = make_float2(0.f, 0.f);
+        vals[j * NPOL + p] = o;
+      }
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+      const VisRec r = recs[j];
+      float2 vv[NPOL];
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) vv[p] = vals[j * NPOL + p];
+      const float2* __restrict__ cfp = a.cf.data + r.cfoff;
+#pragma unroll
+      for (int q = 0; q < MAXSLOTS; ++q) {
+        if (rx[q] < 0) continue;
+        int jx = rx[q] - r.mx;
+        jx += (jx < 0) ? W : 0;
+        int jy = ry[q] - r.my;
+        jy += (jy < 0) ? W : 0;
+        if (jx >= r.w || jy >= r.w) continue;
+        const int cell = (r.px0 + jx) + P * (r.py0 + jy);
+        const float2 c = __ldg(cfp + jx + r.w * jy);
+        if (cell != cur[q]) {
+          if (cur[q] >= 0) {
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+              float2 g = acc_s[p * P2 + cur[q]];
+              g.x += acc[q][p].x;
+              g.y += acc[q][p].y;
+              acc_s[p * P2 + cur[q]] = g;
+              acc[q][p] = make_float2(0.f, 0.f);
+            }
+          }
+          cur[q] = cell;
+        }
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          acc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, acc[q][p].x));
+          acc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, acc[q][p].y));
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < MAXSLOTS; ++q) {
+    if (cur[q] >= 0) {
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float2 g = acc_s[p * P2 + cur[q]];
+        g.x += acc[q][p].x;
+        g.y += acc[q][p].y;
+        acc_s[p * P2 + cur[q]] = g;
+      }
+    }
+  }
+  __syncthreads();
+  float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
+  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) out[i] = acc_s[i];
+}
+
+// ---------------------------------------------------------------------------
+// k_halo_sum: grid[cell] += sum over items whose padded tile covers the cell.
+// One CTA per (grid-plane/channel, tile).  Items of a tile are consecutive.
+// ---------------------------------------------------------------------------
+struct HaloArgs {
+  const int* item_base;      // per tile: first item
+  const int* nit;            // per tile: number of items
+  const float2* scratch;
+  float2* grid;              // ngc planes of (nx, ny, npol) per grid plane
+  int nx, ny, npol, nchan_img;
+  int tile, ntx, nty;
+  long long ntiles;
+  int smax, P;
+};
+
+__global__ void k_halo_sum(HaloArgs a) {
+  const long long tid = blockIdx.x;               // over ngc * ntiles
+  const long long gc = tid / a.ntiles;
+  const long long t = tid % a.ntiles;
+  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
+  const int R = (a.smax + a.tile - 1) / a.tile;   // neighbour reach in tiles
+  // quick exit when no neighbouring tile holds data
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int q = threadIdx.x; q < (2 * R + 1) * (2 * R + 1); q += blockDim.x) {
+    const int ax = tx + q % (2 * R + 1) - R, ay = ty + q / (2 * R + 1) - R;
+    if (ax < 0 || ay < 0 || ax >= a.ntx || ay >= a.nty) continue;
+    if (a.nit[gc * a.ntiles + ax + (long long)a.ntx * ay] > 0) any = 1;
+  }
+  __syncthreads();
+  if (!any) return;
+  const int gind = (int)(gc / a.nchan_img), ichan = (int)(gc % a.nchan_img);
+  const long long plane_cells = (long long)a.nx * a.ny;
+  const int P2 = a.P * a.P;
+  const int T = a.tile;
+  for (int c = threadIdx.x; c < T * T * a.npol; c += blockDim.x) {
+    const int lx = c % T, ly = (c / T) % T, p = c / (T * T);
+    const int x = tx * T + lx, y = ty * T + ly;
+    if (x >= a.nx || y >= a.ny) continue;
+    float2 sum = make_float2(0.f, 0.f);
+    bool hit = false;
+    for (int dy = -R; dy <= R; ++dy) {
+      const int ay = ty + dy;
+      if (ay < 0 || ay >= a.nty) continue;
+      const int py = y - (ay * T - a.smax);
+      if (py < 0 || py >= a.P) continue;
+      for (int dx = -R; dx <= R; ++dx) {
+        const int ax = tx + dx;
+        if (ax < 0 || ax >= a.ntx) continue;
+        const int px = x - (ax * T - a.smax);
+        if (px < 0 || px >= a.P) continue;
+        const long long nt = gc * a.ntiles + ax + (long long)a.ntx * ay;
+        const int m = a.nit[nt];
+        if (m == 0) continue;
+        const int b = a.item_base[nt];
+        for (int j = 0; j < m; ++j) {
+          const float2 v = a.scratch[((size_t)(b + j) * a.npol + p) * P2 + px + (size_t)a.P * py];
+          sum.x += v.x;
+          sum.y += v.y;
+          hit = true;
+        }
+      }
+    }
+    if (hit) {
+      float2* g = a.grid + (size_t)gind * plane_cells * a.npol * a.nchan_img +
+                  plane_cells * (p + (size_t)a.npol * ichan) + x + (size_t)a.nx * y;
+      float2 o = *g;
+      o.x += sum.x;
+      o.y += sum.y;
+      *g = o;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_degrid: vis = sum CF * conj(grid) (GridKernel.cc:99-137), * mfs, * phasor
+// ---------------------------------------------------------------------------
+struct DegridKArgs {
+  const int4* items;
+  const unsigned int* val;
+  const unsigned int* pos;
+  const int* cfi;
+  VisArgs v;
+  CFView cf;
+  const float2* grid;
+  int nx, ny, nchan_img;
+  const int* chan_map;
+  int tile, ntx;
+  long long ntiles;
+  int smax, P;
+  int smem_grid;             // 1: padded tile staged in shared memory
+  float2* out;               // per sample: npol values (sample order)
+};
+
+constexpr int kDegridThreads = 256;
+
+template <int NPOL>
+__global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
+  extern __shared__ float4 smem_raw[];
+  float2* g_s = reinterpret_cast<float2*>(smem_raw);
+  const int4 it = a.items[blockIdx.x];
+  const long long tile_id = it.x;
+  const long long gc = tile_id / a.ntiles;
+  const long long t = tile_id % a.ntiles;
+  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
+  const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
+  const int P = a.P, P2 = P * P;
+  const int gind = (int)(gc / a.nchan_img), ichan = (int)(gc % a.nchan_img);
+  const long long plane_cells = (long long)a.nx * a.ny;
+  const float2* gbase = a.grid + (size_t)gind * plane_cells * NPOL * a.nchan_img + plane_cells * ((size_t)NPOL * ichan);
+  if (a.smem_grid) {
+    for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
+      const int px = i % P, py = (i / P) % P, p = i / P2;
+      const int x = X0 + px, y = Y0 + py;
+      float2 g = make_float2(0.f, 0.f);
+      if (x >= 0 && y >= 0 && x < a.nx && y < a.ny) g = gbase[plane_cells * p + x + (size_t)a.nx * y];
+      g_s[i] = g;
+    }
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const long long n = a.v.nrow * (long long)a.v.nchan;
+  for (int i = it.y + warp; i < it.z; i += nwarps) {
+    const unsigned int s = a.val[i];
+    const unsigned int ps = a.pos[s];
+    const int c = a.cfi[s];
+    const int w = a.cf.size[c];
+    const int sup = (w - 1) / 2;
+    const int px0 = (int)(ps & 0xffffu) - sup - X0;
+    const int py0 = (int)(ps >> 16) - sup - Y0;
+    const float2* __restrict__ cfp = a.cf.data + a.cf.off[c];
+    float re[NPOL], im[NPOL];
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) { re[p] = 0.f; im[p] = 0.f; }
+    const int ntaps = w * w;
+    int jx = lane % w, jy = lane / w;
+    for (int tp = lane; tp < ntaps; tp += 32) {
+      const float2 cv = __ldg(cfp + tp);
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float2 g;
+        if (a.smem_grid) {
+          g = g_s[p * P2 + (px0 + jx) + P * (py0 + jy)];
+        } else {
+          g = __ldg(gbase + plane_cells * p + (X0 + px0 + jx) + (size_t)a.nx * (Y0 + py0 + jy));
+        }
+        re[p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[p]));
+        im[p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[p]));
+      }
+      jx += 32;
+      while (jx >= w) { jx -= w; ++jy; }
+    }
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        re[p] += __shfl_xor_sync(0xffffffffu, re[p], o);
+        im[p] += __shfl_xor_sync(0xffffffffu, im[p], o);
+      }
+    }
+    if (lane == 0) {
+      const long long row = s % a.v.nrow;
+      const int chan = (int)(s / a.v.nrow);
+      float pr, pi;
+      phasor_of(a.v, row, chan, &pr, &pi);
+      const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float cr = re[p], ci = im[p];
+        if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
+        const float orr = __fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi));
+        const float oi = __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr));
+        a.out[(size_t)s * NPOL + p] = make_float2(orr, oi);
+      }
+    }
+  }
+  (void)n;
+}
+
+// prev[o] = o when sample (row, chan) with o = row * nchan + chan is on-grid,
+// -1 otherwise (input of the max-scan)
+__global__ void k_order_marks(const unsigned char* __restrict__ status, long long nrow, int nchan, int want,
+                              int* __restrict__ marks) {
+  const long long n = nrow * (long long)nchan;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / nchan;
+    const int chan = (int)(o % nchan);
+    const long long s = row + nrow * chan;
+    marks[o] = (status[s] >= want) ? (int)o : -1;
+  }
+}
+
+// vis(row, chan, pol) += value; off-grid valid samples receive the value of the
+// most recent on-grid sample in the reference's loop order (row outer, channel
+// inner), or the value carried over from the previous call.
+__global__ void k_degrid_writeback(const unsigned char* __restrict__ status, const int* __restrict__ prev,
+                                   const float2* __restrict__ vals, const float2* __restrict__ carry,
+                                   long long nrow, int nchan, int npol, float2* __restrict__ vis) {
+  const long long n = nrow * (long long)nchan;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / nchan;
+    const int chan = (int)(o % nchan);
+    const long long s = row + nrow * chan;
+    const unsigned char st = status[s];
+    if (st < 2) continue;
+    const int q = prev[o];
+    for (int p = 0; p < npol; ++p) {
+      float2 v;
+      if (q >= 0) {
+        const long long sq = (q / nchan) + nrow * (q % nchan);
+        v = vals[(size_t)sq * npol + p];
+      } else {
+        v = carry[p];
+      }
+      float2 o2 = vis[s + n * p];
+      o2.x += v.x;
+      o2.y += v.y;
+      vis[s + n * p] = o2;
+    }
+  }
+}
+
+// carry_out = value of the last sample in loop order with status >= want
+__global__ void k_update_carry(const int* __restrict__ prev, long long nrow, int nchan, int npol,
+                               const float2* __restrict__ vals, int vals_are_vis, float2* __restrict__ carry) {
+  const long long n = nrow * (long long)nchan;
+  if (n == 0) return;
+  const int q = prev[n - 1];
+  if (q < 0) return;
+  const long long sq = (q / nchan) + nrow * (q % nchan);
+  for (int p = threadIdx.x; p < npol; p += blockDim.x) {
+    carry[p] = vals_are_vis ? vals[sq + n * p] : vals[(size_t)sq * npol + p];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+static inline int grid_dim(long long n, int threads, int cap = 148 * 32) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+static int ceil_log2(unsigned long long v) {
+  int b = 0;
+  while ((1ull << b) < v && b < 63) ++b;
+  return b;
+}
+
+#define YG_CUDA_TRY(x)                          \
+  do {                                          \
+    cudaError_t e_ = (x);                       \
+    if (e_ != cudaSuccess) return YG_ERR_CUDA;  \
+  } while (0)
+
+// Bins one chunk: fills plan (sorted ids, tile table, work items).
+int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st) {
+  const long long n = a.nrow * (long long)a.nchan;
+  pl.nsamples = n;
+  pl.nrow = a.nrow;
+  pl.nchan = a.nchan;
+  pl.npol = a.npol;
+  pl.tile = a.tile;
+  pl.ntx = a.ntx;
+  pl.nty = a.nty;
+  pl.vmax = vmax;
+  pl.smax = (a.cf.maxsize - 1) / 2;
+  pl.pad = a.tile + 2 * pl.smax;
+  int ngrid_planes = 1;
+  if (a.grid_mode == GRID_MODE_WPLANE) ngrid_planes = a.ws.nwplanes;
+  if (a.grid_mode == GRID_MODE_STACK) ngrid_planes = a.ws_stack.nwplanes;
+  pl.ngc = ngrid_planes * a.nchan_img;
+  pl.ntiles_total = (long long)pl.ngc * a.ntx * a.nty;
+  if (n == 0) {
+    pl.nvalid = 0;
+    pl.nitems = 0;
+    return YG_OK;
+  }
+  if (n >= (1ll << 31)) return YG_ERR_ARG;  // cub sizes and tile offsets are int
+  YG_CUDA_TRY(pl.key.ensure(n * 8));
+  YG_CUDA_TRY(pl.key_alt.ensure(n * 8));
+  YG_CUDA_TRY(pl.val.ensure(n * 4));
+  YG_CUDA_TRY(pl.val_alt.ensure(n * 4));
+  YG_CUDA_TRY(pl.pos.ensure(n * 4));
+  YG_CUDA_TRY(pl.cfi.ensure(n * 4));
+  YG_CUDA_TRY(pl.status.ensure(n));
+  k_bin<<<grid_dim(n, 256), 256, 0, st>>>(a, pl.key.as<unsigned long long>(), pl.val.as<unsigned int>(),
+                                          pl.pos.as<unsigned int>(), pl.cfi.as<int>(),
+                                          pl.status.as<unsigned char>(), err);
+  YG_CUDA_TRY(cudaGetLastError());
+  // radix sort over the bits that keys use (the invalid key is one past the
+  // largest valid key, so it sorts last)
+  const int end_bit = std::min(64, ceil_log2(a.invalid_key + 1));
+  size_t tmp = 0;
+  cub::DoubleBuffer<unsigned long long> kb(pl.key.as<unsigned long long>(), pl.key_alt.as<unsigned long long>());
+  cub::DoubleBuffer<unsigned int> vb(pl.val.as<unsigned int>(), pl.val_alt.as<unsigned int>());
+  YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, (int)n, 0, end_bit, st));
+  YG_CUDA_TRY(pl.sort_tmp.ensure(tmp));
+  YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(pl.sort_tmp.p, tmp, kb, vb, (int)n, 0, end_bit, st));
+  if (kb.Current() != pl.key.as<unsigned long long>()) {
+    std::swap(pl.key.p, pl.key_alt.p);
+    std::swap(pl.key.bytes, pl.key_alt.bytes);
+  }
+  if (vb.Current() != pl.val.as<unsigned int>()) {
+    std::swap(pl.val.p, pl.val_alt.p);
+    std::swap(pl.val.bytes, pl.val_alt.bytes);
+  }
+  // tile table
+  const long long nt = pl.ntiles_total;
+  YG_CUDA_TRY(pl.tstart.ensure(nt * 4));
+  YG_CUDA_TRY(pl.tend.ensure(nt * 4));
+  YG_CUDA_TRY(pl.nit.ensure(nt * 4));
+  YG_CUDA_TRY(pl.itembase.ensure((nt + 1) * 4));
+  YG_CUDA_TRY(pl.nvalid_d.ensure(16));
+  YG_CUDA_TRY(cudaMemsetAsync(pl.tstart.p, 0, nt * 4, st));
+  YG_CUDA_TRY(cudaMemsetAsync(pl.tend.p, 0, nt * 4, st));
+  YG_CUDA_TRY(cudaMemsetAsync(pl.nvalid_d.p, 0, 16, st));
+  k_tile_bounds<<<grid_dim(n, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), n, a.mbits, a.cf.ncf,
+                                                  a.invalid_key, pl.tstart.as<int>(), pl.tend.as<int>(),
+                                                  pl.nvalid_d.as<long long>());
+  k_count_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), nt, vmax, pl.nit.as<int>());
+  size_t tmp2 = 0;
+  YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
+  if (tmp2 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp2));
+  YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(pl.sort_tmp.p, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
+  int last_base = 0, last_n = 0;
+  long long nvalid = 0;
+  YG_CUDA_TRY(cudaMemcpyAsync(&last_base, pl.itembase.as<int>() + (nt - 1), 4, cudaMemcpyDeviceToHost, st));
+  YG_CUDA_TRY(cudaMemcpyAsync(&last_n, pl.nit.as<int>() + (nt - 1), 4, cudaMemcpyDeviceToHost, st));
+  YG_CUDA_TRY(cudaMemcpyAsync(&nvalid, pl.nvalid_d.p, 8, cudaMemcpyDeviceToHost, st));
+  YG_CUDA_TRY(cudaStreamSynchronize(st));
+  pl.nitems = last_base + last_n;
+  pl.nvalid = nvalid;
+  YG_CUDA_TRY(pl.items.ensure((size_t)std::max(1, pl.nitems) * sizeof(int4)));
+  k_fill_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), pl.nit.as<int>(),
+                                                  pl.itembase.as<int>(), nt, vmax, pl.items.as<int4>());
+  YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+static int max_slots_for(int W, int threads) { return (W * W + threads - 1) / threads; }
+
+template <int NPOL>
+static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, int slots, cudaStream_t st) {
+  if (slots <= 4) {
+    auto k = k_grid<NPOL, 4>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nitems, kGridThreads, smem, st>>>(g);
+  } else if (slots <= 8) {
+    auto k = k_grid<NPOL, 8>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nitems, kGridThreads, smem, st>>>(g);
+  } else if (slots <= 16) {
+    auto k = k_grid<NPOL, 16>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nitems, kGridThreads, smem, st>>>(g);
+  } else {
+    return cudaErrorInvalidConfiguration;
+  }
+  return cudaGetLastError();
+}
+
+size_t grid_smem_bytes(int npol, int P) {
+  return (size_t)npol * P * P * sizeof(float2) + kBatch * sizeof(VisRec) + (size_t)kBatch * npol * sizeof(float2);
+}
+
+// Polarisations accumulated together in one k_grid pass: the most that fit
+// the shared-memory budget.
+int grid_pols_per_pass(int npol, int P) {
+  const int cands[3] = {4, 2, 1};
+  for (int c : cands) {
+    if (c > npol || npol % c) continue;
+    if (grid_smem_bytes(c, P) <= 227 * 1024) return c;
+  }
+  return 0;
+}
+
+// Grids the samples of a plan onto `grid` (ngrid planes of (nx, ny, npol, nchan_img)).
+int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
+              DevBuf& scratch, DevError* err, cudaStream_t st) {
+  if (pl.nitems == 0) return YG_OK;
+  const int P = pl.pad;
+  const int W = 2 * pl.smax + 1;
+  const int slots = max_slots_for(W, kGridThreads);
+  const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
+  YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
+  GridKArgs g;
+  g.items = pl.items.as<int4>();
+  g.val = pl.val.as<unsigned int>();
+  g.pos = pl.pos.as<unsigned int>();
+  g.cfi = pl.cfi.as<int>();
+  g.v = v;
+  g.cf = cf;
+  g.tile = pl.tile;
+  g.ntx = pl.ntx;
+  g.ntiles = (long long)pl.ntx * pl.nty;
+  g.smax = pl.smax;
+  g.P = P;
+  g.scratch = scratch.as<float2>();
+  g.npol_total = v.npol;
+  g.err = err;
+  const int npa = grid_pols_per_pass(v.npol, P);
+  if (npa == 0) return YG_ERR_UNSUPPORTED;
+  const size_t smem = grid_smem_bytes(npa, P);
+  for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
+    g.pol0 = pol0;
+    cudaError_t e;
+    switch (npa) {
+      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, slots, st); break;
+      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, slots, st); break;
+      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, slots, st); break;
+      default: return YG_ERR_UNSUPPORTED;
+    }
+    if (e != cudaSuccess) return YG_ERR_CUDA;
+  }
+  HaloArgs h;
+  h.item_base = pl.itembase.as<int>();
+  h.nit = pl.nit.as<int>();
+  h.scratch = scratch.as<float2>();
+  h.grid = grid;
+  h.nx = nx;
+  h.ny = ny;
+  h.npol = v.npol;
+  h.nchan_img = nchan_img;
+  h.tile = pl.tile;
+  h.ntx = pl.ntx;
+  h.nty = pl.nty;
+  h.ntiles = (long long)pl.ntx * pl.nty;
+  h.smax = pl.smax;
+  h.P = P;
+  const long long nblocks = pl.ntiles_total;
+  if (nblocks > 0x7fffffffll) return YG_ERR_UNSUPPORTED;
+  k_halo_sum<<<(unsigned)nblocks, 256, 0, st>>>(h);
+  YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
+              int nchan_img, double* sumw, DevError* err, cudaStream_t st) {
+  if (pl.nsamples == 0) return YG_OK;
+  k_sumw<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, pl.status.as<unsigned char>(), pl.cfi.as<int>(), chan_map,
+                                                     os, track_per_os, nrows_sumw, nchan_img, sumw, err);
+  YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+// Degrids the samples of a plan from `grid` and adds the result into vis.
+int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
+                int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
+                cudaStream_t st) {
+  const long long n = pl.nsamples;
+  if (n == 0) return YG_OK;
+  YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
+  if (pl.nitems > 0) {
+    DegridKArgs d;
+    d.items = pl.items.as<int4>();
+    d.val = pl.val.as<unsigned int>();
+    d.pos = pl.pos.as<unsigned int>();
+    d.cfi = pl.cfi.as<int>();
+    d.v = v;
+    d.cf = cf;
+    d.grid = grid;
+    d.nx = nx;
+    d.ny = ny;
+    d.nchan_img = nchan_img;
+    d.chan_map = chan_map;
+    d.tile = pl.tile;
+    d.ntx = pl.ntx;
+    d.ntiles = (long long)pl.ntx * pl.nty;
+    d.smax = pl.smax;
+    d.P = pl.pad;
+    d.out = tmp_vals.as<float2>();
+    size_t smem = (size_t)v.npol * pl.pad * pl.pad * sizeof(float2);
+    d.smem_grid = smem <= 200 * 1024 ? 1 : 0;
+    if (!d.smem_grid) smem = 0;
+    cudaError_t e = cudaSuccess;
+    switch (v.npol) {
+      case 1: {
+        auto k = k_degrid<1>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        break;
+      }
+      case 2: {
+        auto k = k_degrid<2>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        break;
+      }
+      case 4: {
+        auto k = k_degrid<4>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        break;
+      }
+      default:
+        return YG_ERR_UNSUPPORTED;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return YG_ERR_CUDA;
+  }
+  // write-back with the reference's carried value for off-grid samples
+  YG_CUDA_TRY(pl.order_prev.ensure((size_t)n * 4 * 2));
+  int* marks = pl.order_prev.as<int>();
+  int* prev = marks + n;
+  k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 3, marks);
+  size_t tmp = 0;
+  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
+  YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
+  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
+  k_degrid_writeback<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), prev, tmp_vals.as<float2>(),
+                                                       carry, pl.nrow, pl.nchan, v.npol, vis_out);
+  k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, tmp_vals.as<float2>(), 0, carry);
+  YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+// grid mode: itsImagePolFrameVis ends as the last used (flag-free, mapped)
+// sample's visibility in loop order.
+int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st) {
+  const long long n = pl.nsamples;
+  if (n == 0 || v.psf) return YG_OK;
+  YG_CUDA_TRY(pl.order_prev.ensure((size_t)n * 4 * 2));
+  int* marks = pl.order_prev.as<int>();
+  int* prev = marks + n;
+  k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 1, marks);
+  size_t tmp = 0;
+  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
+  YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
+  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
+  k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, v.vis, 1, carry);
+  YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+}  // namespace yg

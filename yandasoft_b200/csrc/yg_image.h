@@ -1,0 +1,35 @@
+// Image-side FFT steps (finaliseGrid / initialiseDegrid) on the GPU.
+#pragma once
+#include <cufft.h>
+
+#include <vector>
+
+#include "yg_internal.h"
+
+namespace yg {
+
+struct StackScreen {
+  int nx, ny;
+  float cellx, celly;   // FP32 image cell (radians), as WStackVisGridder::multiply
+  float w;              // FP32 2 pi w
+};
+
+StackScreen make_stack_screen(int nx, int ny, double uvcell_u, double uvcell_v, double wterm);
+
+struct ImageFFT {
+  cufftHandle plan = 0;
+  bool plan_ok = false;
+  int nx = 0, ny = 0, nplanes = 0;
+  DevBuf work;
+  int ensure(int nx, int ny, int nplanes, cudaStream_t st);
+  ~ImageFFT();
+};
+
+int image_finalise(ImageFFT& f, const float2* grids, int ngrids, int nx, int ny, int nplanes,
+                   const std::vector<StackScreen>* screens, const double* corr_x, const double* corr_y, float* out,
+                   cudaStream_t st);
+int image_to_grids(ImageFFT& f, const float* image, int nx, int ny, int nplanes,
+                   const std::vector<StackScreen>* screens, int ngrids, const double* corr_x, const double* corr_y,
+                   float* corrected_tmp, float2* grids, cudaStream_t st);
+
+}  // namespace yg

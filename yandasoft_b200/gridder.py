@@ -1,0 +1,408 @@
+"""Python binding of the B200 gridder's C-ABI (include/yg.h).
+
+Mirrors yandasoft's gridder interface so that callers and tests read like the
+reference's own: ``VisGridderFactory.make(parset)`` returns an ``IVisGridder``
+with ``initialiseGrid / grid / finaliseGrid / finaliseWeights /
+initialiseDegrid / degrid / finaliseDegrid / customiseForContext /
+initVisWeights / isModelEmpty / clone`` (askap/gridding/IVisGridder.h:64-140,
+VisGridderFactory.cc:112-285).  Failures raise ``AskapError`` carrying the
+library's status code, as ASKAPCHECK throws in the reference.
+
+The CUDA library must be built (``yandasoft_b200.build``); there is no CPU
+fallback: without the extension every call fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libyg_b200.so")
+_LIB = None
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+I64 = ctypes.c_int64
+D = ctypes.c_double
+
+# names exported by include/yg.h
+EXPORTS = [
+    "yg_last_error", "yg_create", "yg_clone", "yg_destroy", "yg_initialise_grid", "yg_grid", "yg_finalise_grid",
+    "yg_finalise_weights", "yg_initialise_degrid", "yg_degrid", "yg_finalise_degrid", "yg_customise_for_context",
+    "yg_init_vis_weights_mfs", "yg_is_model_empty", "yg_get_support", "yg_get_cf", "yg_get_cf_offsets",
+    "yg_get_sum_weights", "yg_get_grid", "yg_get_shape", "yg_get_stats", "yg_build_cf", "yg_plan_create",
+    "yg_plan_grid", "yg_plan_degrid", "yg_plan_info", "yg_plan_samples", "yg_plan_destroy", "yg_set_tile", "yg_set_item_size",
+    "yg_synchronize",
+]
+
+
+class AskapError(RuntimeError):
+    """Error raised by the gridder (status code in ``.code``)."""
+
+    def __init__(self, code, msg):
+        super().__init__("%s (code %d)" % (msg, code))
+        self.code = code
+
+
+class yg_axes(ctypes.Structure):
+    _fields_ = [("cell", D * 2), ("centre", D * 2), ("tangent", D * 2), ("has_freq", I32), ("reserved", I32),
+                ("freq_start", D), ("freq_end", D)]
+
+
+class yg_chunk(ctypes.Structure):
+    _fields_ = [("nrow", I64), ("nchan", I32), ("npol", I32), ("uvw", P), ("delay", P), ("freq", P), ("vis", P),
+                ("noise", P), ("flag", P), ("feed1", P), ("pointing", P), ("on_device", I32), ("reserved", I32)]
+
+
+def load(path: str | None = None):
+    """Loads libyg_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    p = path or LIBPATH
+    if not os.path.exists(p):
+        raise AskapError(2, "CUDA gridder library %s is missing: run yandasoft_b200.build.build()" % p)
+    L = ctypes.CDLL(p)
+    L.yg_last_error.restype = ctypes.c_char_p
+    L.yg_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(P)]
+    L.yg_clone.argtypes = [P, ctypes.POINTER(P)]
+    L.yg_destroy.argtypes = [P]
+    L.yg_destroy.restype = None
+    L.yg_initialise_grid.argtypes = [P, ctypes.POINTER(yg_axes), I32, I32, I32, I32, I32, I32]
+    L.yg_grid.argtypes = [P, ctypes.POINTER(yg_chunk)]
+    L.yg_finalise_grid.argtypes = [P, P, I32]
+    L.yg_finalise_weights.argtypes = [P, P, I32]
+    L.yg_initialise_degrid.argtypes = [P, ctypes.POINTER(yg_axes), I32, I32, I32, I32, P, I32]
+    L.yg_degrid.argtypes = [P, ctypes.POINTER(yg_chunk)]
+    L.yg_finalise_degrid.argtypes = [P]
+    L.yg_customise_for_context.argtypes = [P, ctypes.c_char_p]
+    L.yg_init_vis_weights_mfs.argtypes = [P, D]
+    L.yg_is_model_empty.argtypes = [P, ctypes.POINTER(I32)]
+    L.yg_get_support.argtypes = [P, ctypes.POINTER(I32), ctypes.POINTER(I32), ctypes.POINTER(I32)]
+    L.yg_get_cf.argtypes = [P, P, P, P, I64]
+    L.yg_get_cf_offsets.argtypes = [P, P, I32, ctypes.POINTER(I32)]
+    L.yg_get_sum_weights.argtypes = [P, P, I64, ctypes.POINTER(I32)]
+    L.yg_get_grid.argtypes = [P, P, I64, ctypes.POINTER(I32)]
+    L.yg_get_shape.argtypes = [P] + [ctypes.POINTER(I32)] * 4
+    L.yg_get_stats.argtypes = [P, P]
+    L.yg_build_cf.argtypes = [P]
+    L.yg_plan_create.argtypes = [P, ctypes.POINTER(yg_chunk), ctypes.POINTER(P)]
+    L.yg_plan_grid.argtypes = [P, P, ctypes.POINTER(yg_chunk)]
+    L.yg_plan_degrid.argtypes = [P, P, ctypes.POINTER(yg_chunk)]
+    L.yg_plan_info.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
+    L.yg_plan_samples.argtypes = [P, P, P, P, P, P]
+    L.yg_plan_destroy.argtypes = [P]
+    L.yg_plan_destroy.restype = None
+    L.yg_set_tile.argtypes = [P, I32]
+    L.yg_set_item_size.argtypes = [P, I32]
+    L.yg_synchronize.argtypes = [P]
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise AskapError(rc, load().yg_last_error().decode())
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+@dataclass
+class Axes:
+    """Image axes: direction increments (rad), image centre and tangent point,
+    optional FREQUENCY axis (start, end) in Hz."""
+    cell_x: float
+    cell_y: float
+    centre: tuple = (0.0, 0.0)
+    tangent: tuple = (0.0, 0.0)
+    freq: tuple | None = None
+
+    def c(self):
+        a = yg_axes()
+        a.cell[0], a.cell[1] = self.cell_x, self.cell_y
+        a.centre[0], a.centre[1] = self.centre
+        a.tangent[0], a.tangent[1] = self.tangent
+        if self.freq is not None:
+            a.has_freq = 1
+            a.freq_start, a.freq_end = self.freq
+        return a
+
+
+class Accessor:
+    """A chunk of visibilities (IConstDataAccessor / IDataAccessor unpacked).
+
+    numpy arrays (host) or torch CUDA tensors (device).  Cubes are
+    (nrow, nchan, npol) complex64 in Fortran order (row fastest)."""
+
+    def __init__(self, uvw, freq, vis, noise=None, flag=None, delay=None, feed1=None, pointing=None, shape=None):
+        self.uvw, self.freq, self.vis = uvw, freq, vis
+        self.noise, self.flag, self.delay, self.feed1, self.pointing = noise, flag, delay, feed1, pointing
+        self.on_device = hasattr(vis, "data_ptr")
+        if not self.on_device:
+            self.uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+            self.freq = np.ascontiguousarray(freq, dtype=np.float64)
+            if not (vis.dtype == np.complex64 and vis.flags.f_contiguous):
+                raise AskapError(1, "vis must be a Fortran-ordered complex64 cube")
+            if noise is not None:
+                self.noise = np.asfortranarray(noise, dtype=np.complex64)
+            if flag is not None:
+                self.flag = np.asfortranarray(flag.astype(np.uint8))
+            if delay is not None:
+                self.delay = np.ascontiguousarray(delay, dtype=np.float64)
+            if feed1 is not None:
+                self.feed1 = np.ascontiguousarray(feed1, dtype=np.int32)
+        if pointing is not None:
+            self.pointing = np.ascontiguousarray(pointing, dtype=np.float64)
+        shp = tuple(shape) if shape is not None else tuple(vis.shape)
+        self.nrow, self.nchan, self.npol = shp
+
+    def to_device(self, device="cuda"):
+        """Copy of this host accessor with every array in torch device memory
+        (same memory layout; cubes stay column-major)."""
+        import torch
+
+        def dev(a, dt=None):
+            if a is None:
+                return None
+            a = np.asarray(a)
+            flat = a.ravel(order="K") if (a.flags.f_contiguous or a.flags.c_contiguous) else a.ravel(order="F")
+            if np.iscomplexobj(flat):
+                flat = flat.view(np.float32 if flat.dtype == np.complex64 else np.float64)
+            return torch.from_numpy(np.ascontiguousarray(flat)).to(device)
+
+        return Accessor(dev(self.uvw), dev(self.freq), dev(self.vis), noise=dev(self.noise), flag=dev(self.flag),
+                        delay=dev(self.delay), feed1=dev(self.feed1), pointing=self.pointing,
+                        shape=(self.nrow, self.nchan, self.npol))
+
+    def vis_numpy(self):
+        """The visibility cube as a (nrow, nchan, npol) complex64 Fortran array."""
+        if not self.on_device:
+            return self.vis
+        flat = self.vis.detach().cpu().numpy().view(np.complex64)
+        return flat.reshape((self.nrow, self.nchan, self.npol), order="F")
+
+    def c(self):
+        c = yg_chunk()
+        c.nrow, c.nchan, c.npol = self.nrow, self.nchan, self.npol
+        c.uvw, c.delay, c.freq = _ptr(self.uvw), _ptr(self.delay), _ptr(self.freq)
+        c.vis, c.noise, c.flag = _ptr(self.vis), _ptr(self.noise), _ptr(self.flag)
+        c.feed1 = _ptr(self.feed1)
+        c.pointing = None if self.pointing is None else self.pointing.ctypes.data
+        c.on_device = 1 if self.on_device else 0
+        return c
+
+
+class Plan:
+    def __init__(self, gridder, acc: Accessor):
+        self._lib = load()
+        self.h = P()
+        self._chunk = acc.c()
+        _check(self._lib.yg_plan_create(gridder.h, ctypes.byref(self._chunk), ctypes.byref(self.h)))
+
+    def samples(self, gridder, acc: "Accessor"):
+        """(iu, iv, cfi, status) per sample, (nrow, nchan) Fortran arrays."""
+        n = acc.nrow * acc.nchan
+        iu = np.zeros(n, dtype=np.int32)
+        iv = np.zeros(n, dtype=np.int32)
+        c = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.uint8)
+        _check(self._lib.yg_plan_samples(gridder.h, self.h, iu.ctypes.data, iv.ctypes.data, c.ctypes.data,
+                                         st.ctypes.data))
+        shp = (acc.nrow, acc.nchan)
+        return (iu.reshape(shp, order="F"), iv.reshape(shp, order="F"), c.reshape(shp, order="F"),
+                st.reshape(shp, order="F"))
+
+    def info(self):
+        nv, ni, t = I64(), I32(), I32()
+        _check(self._lib.yg_plan_info(self.h, ctypes.byref(nv), ctypes.byref(ni), ctypes.byref(t)))
+        return dict(nvalid=nv.value, nitems=ni.value, tile=t.value)
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            self._lib.yg_plan_destroy(self.h)
+            self.h = P()
+
+
+class IVisGridder:
+    """Handle on one gridder instance (owns a CUDA stream and device memory)."""
+
+    def __init__(self, handle):
+        self._lib = load()
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            self._lib.yg_destroy(self.h)
+            self.h = P()
+
+    def clone(self) -> "IVisGridder":
+        out = P()
+        _check(self._lib.yg_clone(self.h, ctypes.byref(out)))
+        return IVisGridder(out)
+
+    # ---- gridding ----
+    def initialiseGrid(self, axes: Axes, shape, dopsf=False, dopcf=False):
+        nx, ny, npol, nchan = shape
+        self._shape = tuple(shape)
+        _check(self._lib.yg_initialise_grid(self.h, ctypes.byref(axes.c()), nx, ny, npol, nchan, int(dopsf), int(dopcf)))
+
+    def grid(self, acc: Accessor):
+        c = acc.c()
+        _check(self._lib.yg_grid(self.h, ctypes.byref(c)))
+
+    def finaliseGrid(self, out=None):
+        nx, ny, npol, nchan = self._shape
+        if out is None:
+            out = np.zeros((nx, ny, npol, nchan), dtype=np.float32, order="F")
+        on_dev = 1 if hasattr(out, "data_ptr") else 0
+        _check(self._lib.yg_finalise_grid(self.h, _ptr(out), on_dev))
+        return out
+
+    def finaliseWeights(self, out=None):
+        nx, ny, npol, nchan = self._shape
+        if out is None:
+            out = np.zeros((nx, ny, npol, nchan), dtype=np.float32, order="F")
+        _check(self._lib.yg_finalise_weights(self.h, _ptr(out), 1 if hasattr(out, "data_ptr") else 0))
+        return out
+
+    # ---- degridding ----
+    def initialiseDegrid(self, axes: Axes, image):
+        if hasattr(image, "data_ptr"):
+            nx, ny, npol, nchan = image.shape_fortran if hasattr(image, "shape_fortran") else image.shape
+            on_dev = 1
+        else:
+            image = np.asfortranarray(image, dtype=np.float32)
+            nx, ny, npol, nchan = image.shape
+            on_dev = 0
+        self._shape = (nx, ny, npol, nchan)
+        self._model = image
+        _check(self._lib.yg_initialise_degrid(self.h, ctypes.byref(axes.c()), nx, ny, npol, nchan, _ptr(image), on_dev))
+
+    def degrid(self, acc: Accessor):
+        c = acc.c()
+        _check(self._lib.yg_degrid(self.h, ctypes.byref(c)))
+
+    def finaliseDegrid(self):
+        _check(self._lib.yg_finalise_degrid(self.h))
+
+    def customiseForContext(self, context: str):
+        _check(self._lib.yg_customise_for_context(self.h, context.encode()))
+
+    def initVisWeights(self, reffreq: float):
+        """VisWeightsMultiFrequency(reffreq)."""
+        _check(self._lib.yg_init_vis_weights_mfs(self.h, float(reffreq)))
+
+    def isModelEmpty(self) -> bool:
+        v = I32()
+        _check(self._lib.yg_is_model_empty(self.h, ctypes.byref(v)))
+        return bool(v.value)
+
+    # ---- plans (repeated passes over resident data) ----
+    def plan(self, acc: Accessor) -> Plan:
+        return Plan(self, acc)
+
+    def grid_plan(self, plan: Plan, acc: Accessor):
+        c = acc.c()
+        _check(self._lib.yg_plan_grid(self.h, plan.h, ctypes.byref(c)))
+
+    def degrid_plan(self, plan: Plan, acc: Accessor):
+        c = acc.c()
+        _check(self._lib.yg_plan_degrid(self.h, plan.h, ctypes.byref(c)))
+
+    def synchronize(self):
+        _check(self._lib.yg_synchronize(self.h))
+
+    def set_tile(self, t: int):
+        _check(self._lib.yg_set_tile(self.h, int(t)))
+
+    def set_item_size(self, v: int):
+        _check(self._lib.yg_set_item_size(self.h, int(v)))
+
+    # ---- inspection ----
+    def support(self):
+        s, o, n = I32(), I32(), I32()
+        _check(self._lib.yg_get_support(self.h, ctypes.byref(s), ctypes.byref(o), ctypes.byref(n)))
+        return s.value, o.value, n.value
+
+    def build_cf(self):
+        _check(self._lib.yg_build_cf(self.h))
+
+    def convolution_functions(self):
+        """List of CF matrices (complex64 [x, y]) indexed like itsConvFunc."""
+        _, _, ncf = self.support()
+        sizes = np.zeros(ncf, dtype=np.int32)
+        offs = np.zeros(ncf, dtype=np.int64)
+        _check(self._lib.yg_get_cf(self.h, sizes.ctypes.data, offs.ctypes.data, None, 0))
+        total = int(np.sum(sizes.astype(np.int64) ** 2))
+        data = np.zeros(total, dtype=np.complex64)
+        _check(self._lib.yg_get_cf(self.h, sizes.ctypes.data, offs.ctypes.data, data.ctypes.data, total))
+        out = []
+        for i in range(ncf):
+            n = int(sizes[i])
+            out.append(None if n == 0 else data[offs[i]:offs[i] + n * n].reshape((n, n), order="F"))
+        return out
+
+    def cf_offsets(self):
+        n = I32()
+        _check(self._lib.yg_get_cf_offsets(self.h, None, 0, ctypes.byref(n)))
+        buf = np.zeros(2 * max(1, n.value), dtype=np.int32)
+        _check(self._lib.yg_get_cf_offsets(self.h, buf.ctypes.data, n.value, ctypes.byref(n)))
+        return [tuple(buf[2 * i:2 * i + 2]) for i in range(n.value)]
+
+    def sum_weights(self):
+        rows = I32()
+        _check(self._lib.yg_get_sum_weights(self.h, None, 0, ctypes.byref(rows)))
+        nx, ny, npol, nchan = self.shape()
+        out = np.zeros((rows.value, npol, nchan), dtype=np.float64, order="F")
+        _check(self._lib.yg_get_sum_weights(self.h, out.ctypes.data, out.size, ctypes.byref(rows)))
+        return out
+
+    def shape(self):
+        a, b, c, d = I32(), I32(), I32(), I32()
+        _check(self._lib.yg_get_shape(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
+
+    def grids(self):
+        n = I32()
+        _check(self._lib.yg_get_grid(self.h, None, 0, ctypes.byref(n)))
+        nx, ny, npol, nchan = self.shape()
+        buf = np.zeros(n.value * nx * ny * npol * nchan, dtype=np.complex64)
+        _check(self._lib.yg_get_grid(self.h, buf.ctypes.data, buf.size, ctypes.byref(n)))
+        per = nx * ny * npol * nchan
+        return [buf[i * per:(i + 1) * per].reshape((nx, ny, npol, nchan), order="F") for i in range(n.value)]
+
+    def stats(self):
+        out = np.zeros(8)
+        _check(self._lib.yg_get_stats(self.h, out.ctypes.data))
+        keys = ["samples_gridded", "taps_gridded", "samples_degridded", "taps_degridded", "ms_grid", "ms_degrid",
+                "ms_cf", "cf_planes"]
+        return dict(zip(keys, out.tolist()))
+
+
+class VisGridderFactory:
+    @staticmethod
+    def make(parset) -> IVisGridder:
+        """parset: dict or 'key = value' text (keys as in a cimager parset)."""
+        if isinstance(parset, dict):
+            text = "\n".join("%s = %s" % (k, _fmt(v)) for k, v in parset.items())
+        else:
+            text = parset
+        lib = load()
+        h = P()
+        _check(lib.yg_create(text.encode(), ctypes.byref(h)))
+        return IVisGridder(h)
+
+
+def _fmt(v):
+    if isinstance(v, bool):
+        return "true" if v else "false"
+    return str(v)
