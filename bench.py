@@ -1,0 +1,504 @@
+#!/usr/bin/env python
+"""Benchmark: grid+degrid visibility throughput on one B200 (Mvis/s).
+
+One step = one degrid pass (model -> visibilities) plus one grid pass
+(visibilities -> grid) over every visibility sample of the workload: the
+major-cycle shape of ImageFFTEquation::calcImagingEquations.  A visibility
+sample is one (row, channel, polarisation).
+
+Workloads (seeded synthetic data with the shapes of the benchmark configs):
+  --config 1  W-stacking + W-projection, full-track continuum: 36 antennas in a
+              6 km disk, 8 h at 5 s, 96 channels 700-1000 MHz, 4 polarisations
+              (348,364,800 rows x channels, 1.39e9 samples, 11 GB), 4096^2 x 4
+              grid at 4", 17 w-stacks x 33 w-planes, oversample 8.  Default.
+  --config 0  WProject: 36 antennas, 1 h at 10 s, 8 channels 940-948 MHz, XX,
+              2048^2 at 8", 65 w-planes, oversample 4.
+
+`value` is measured with inputs resident in HBM (plan-based passes on device
+buffers); `e2e` goes through the C-ABI IVisGridder calls with pinned host
+buffers, copies included.  `--impl reference` times the CPU restatement of the
+reference gridder (oracle/, single-threaded gridder per host thread over
+channel slices, as the reference runs one gridder per thread or rank).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ARCSEC = math.pi / (180 * 3600)
+C_LIGHT = 299792458.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# workloads
+# --------------------------------------------------------------------------
+def workload(cfg: int, scale: float = 1.0):
+    if cfg == 0:
+        return dict(name="config0_wproject_2048", gridder="WProject", nant=36, diameter=6000.0, lat=-26.7, dec=-45.0,
+                    duration=3600.0 * scale, dt=10.0, f0=940e6, f1=948e6, nchan=8, npol=1, nsrc=20, ngauss=0,
+                    field=2.0, sigma=0.01, nx=2048, cell=8.0, nwplanes=65, oversample=4, cutoff=1e-3,
+                    maxsupport=1024, seed=0)
+    return dict(name="config1_wstack17_wproject33_4096x4pol", gridder="WStackWProject", nant=36, diameter=6000.0,
+                lat=-26.7, dec=-45.0, duration=8 * 3600.0 * scale, dt=5.0, f0=700e6, f1=1000e6, nchan=96, npol=4,
+                nsrc=200, ngauss=10, field=2.0, sigma=0.01, nx=4096, cell=4.0, nwstacks=17, nwplanes=33, oversample=8,
+                cutoff=1e-3, maxsupport=512, seed=1)
+
+
+def gen_device(w):
+    """Synthetic data in HBM (torch).  uvw from the hour-angle rotation, FP64;
+    visibilities from the point/Gaussian measurement equation (phase reduced
+    in FP64, sin/cos in FP32), noise N(0, sigma)."""
+    import torch
+    from yandasoft_b200 import simulate
+    arr = simulate.random_disk_array(w["nant"], w["diameter"], w["lat"], w["seed"])
+    uvw, ntime, nbl = simulate.uvw_track(arr, w["dec"] * simulate.DEG, w["duration"], w["dt"])
+    nchan, npol = w["nchan"], w["npol"]
+    df = (w["f1"] - w["f0"]) / nchan
+    freq = w["f0"] + (np.arange(nchan) + 0.5) * df
+    sky = simulate.random_point_sky(w["nsrc"], w["field"], w["seed"] + 1)
+    comp = sky.components.copy()
+    if w["ngauss"]:
+        rng = np.random.default_rng(w["seed"] + 3)
+        g = rng.choice(len(comp), w["ngauss"], replace=False)
+        comp[g, 3] = rng.uniform(10, 60, len(g)) * ARCSEC   # FWHM major
+        comp[g, 4] = comp[g, 3] * rng.uniform(0.3, 1.0, len(g))
+        comp[g, 5] = rng.uniform(0, math.pi, len(g))
+    dev = torch.device("cuda")
+    nrow = uvw.shape[0]
+    U = torch.from_numpy(uvw).to(dev)
+    F = torch.from_numpy(freq).to(dev)
+    l = torch.from_numpy(comp[:, 1]).to(dev)
+    m = torch.from_numpy(comp[:, 2]).to(dev)
+    flux = torch.from_numpy(comp[:, 0]).to(dev)
+    n = torch.sqrt(1 - l * l - m * m)
+    gauss = torch.from_numpy((comp[:, 3] > 0) | (comp[:, 4] > 0)).to(dev)
+    bmaj = torch.from_numpy(comp[:, 3]).to(dev)
+    bmin = torch.from_numpy(comp[:, 4]).to(dev)
+    bpa = torch.from_numpy(comp[:, 5]).to(dev)
+    scale_g = math.pi ** 2 / (4 * math.log(2.0))
+    model = torch.empty((nchan, nrow), dtype=torch.complex64, device=dev)   # transposed for coalescing
+    R = 1 << 16
+    for r0 in range(0, nrow, R):
+        r1 = min(nrow, r0 + R)
+        u, v, ww = U[r0:r1, 0:1], U[r0:r1, 1:2], U[r0:r1, 2:3]
+        cyc = (l[None] * u + m[None] * v + (n[None] - 1) * ww) / C_LIGHT       # cycles per Hz (FP64)
+        r = None
+        if bool(gauss.any()):
+            up = (torch.cos(bpa)[None] * u + torch.sin(bpa)[None] * v) / C_LIGHT
+            vp = (-torch.sin(bpa)[None] * u + torch.cos(bpa)[None] * v) / C_LIGHT
+            r = (bmaj[None] ** 2 * up * up + bmin[None] ** 2 * vp * vp) * scale_g
+        for c in range(nchan):
+            f = float(freq[c])
+            ph = cyc * f
+            ph = (ph - torch.floor(ph)).float() * (2 * math.pi)
+            amp = flux[None].expand_as(ph)
+            if r is not None:
+                amp = amp * torch.exp(-r * f * f)
+            amp = amp.float()
+            re = (amp * torch.cos(ph)).sum(1)
+            im = (amp * torch.sin(ph)).sum(1)
+            model[c, r0:r1] = torch.complex(re, im)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(w["seed"] + 2)
+    # cube (nrow, nchan, npol) column-major == memory [pol][chan][row]
+    vis = torch.empty((npol, nchan, nrow), dtype=torch.complex64, device=dev)
+    for p in range(npol):
+        sig = model if (npol == 1 or p in (0, npol - 1)) else 0
+        nz = torch.complex(torch.randn((nchan, nrow), generator=gen, device=dev),
+                           torch.randn((nchan, nrow), generator=gen, device=dev)) * w["sigma"]
+        vis[p] = sig + nz
+    del model
+    wmax_data = float(torch.max(torch.abs(U[:, 2]))) * float(freq.max()) / C_LIGHT
+    return dict(uvw=U, freq=F, vis=vis, nrow=nrow, nchan=nchan, npol=npol, freq_np=freq, uvw_np=uvw, sky=comp,
+                wmax=math.ceil(wmax_data * 1.02 / 100.0) * 100.0)
+
+
+def parset_for(w, wmax):
+    g = w["gridder"]
+    p = {"gridder": g, "gridder.%s.wmax" % g: wmax, "gridder.%s.nwplanes" % g: w["nwplanes"],
+         "gridder.%s.oversample" % g: w["oversample"], "gridder.%s.cutoff" % g: w["cutoff"],
+         "gridder.%s.maxsupport" % g: w["maxsupport"]}
+    if g == "WStackWProject":
+        p["gridder.%s.nwstacks" % g] = w["nwstacks"]
+    return p
+
+
+def model_image(w, sky, npol):
+    nx = w["nx"]
+    cell = w["cell"] * ARCSEC
+    img = np.zeros((nx, nx, npol, 1), dtype=np.float32, order="F")
+    for k in range(len(sky)):
+        x = int(round(nx // 2 + sky[k, 1] / cell))
+        y = int(round(nx // 2 + sky[k, 2] / cell))
+        if 0 <= x < nx and 0 <= y < nx:
+            img[x, y, 0, 0] += sky[k, 0]
+            if npol > 1:
+                img[x, y, npol - 1, 0] += sky[k, 0]
+    return img
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0:
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, nm in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# CPU baseline (oracle restatement), bounded sample
+# --------------------------------------------------------------------------
+def cpu_baseline(w, d, target_s=15.0, threads=None):
+    """Times the oracle's C restatement of TableVisGridder::generic on a row
+    subset of the same workload: one degrid + one grid pass.  Threads run
+    independent gridders over channel slices.  Returns (Mvis/s, info)."""
+    import concurrent.futures as cf
+    import oracle
+    from oracle import cf as cfmod
+    threads = threads or (os.cpu_count() or 1)
+    nx = w["nx"]
+    cell = w["cell"] * ARCSEC
+    kind = w["gridder"]
+    kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
+              maxsupport=w["maxsupport"])
+    if kind == "WStackWProject":
+        kw["nwstacks"] = w["nwstacks"]
+    g0 = oracle.OracleGridder(kind, **kw)
+    g0.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+    g0.init_cf()
+    nrow_all = d["nrow"]
+    freq = d["freq_np"]
+    vis_all = d["vis"]
+    # calibrate a row count: ~2 ns per tap per pass, two passes
+    taps = (2 * g0.cache.support + 1) ** 2
+    per_sample = 2 * taps * d["npol"] * 2.0e-9 / max(1, threads)
+    nrows = int(min(nrow_all, max(1000, target_s / (per_sample * len(freq)))))
+    step = max(1, nrow_all // nrows)
+    rows = np.arange(0, nrow_all, step)[:nrows]
+    uvw = np.ascontiguousarray(d["uvw_np"][rows])
+    import torch
+    vis = vis_all[:, :, rows].cpu().numpy()          # [pol][chan][row]
+    cube = np.asfortranarray(np.transpose(vis, (2, 1, 0)))
+    model = model_image(w, d["sky"], d["npol"])
+    slices = np.array_split(np.arange(len(freq)), threads)
+
+    def work(ch):
+        if len(ch) == 0:
+            return 0
+        gd = oracle.OracleGridder(kind, **kw)
+        gd.cache = g0.cache
+        gd._flat = g0._flat
+        gd.initialise_degrid(model, cell, cell)
+        gd.cache = g0.cache
+        gd._flat = g0._flat
+        sub = np.asfortranarray(cube[:, ch, :])
+        out = np.zeros_like(sub)
+        gd.degrid(oracle.Chunk(uvw=uvw, freq=freq[ch], vis=out))
+        gg = oracle.OracleGridder(kind, **kw)
+        gg.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+        gg.cache = g0.cache
+        gg._flat = g0._flat
+        gg.grid(oracle.Chunk(uvw=uvw, freq=freq[ch], vis=sub))
+        return sub.size
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        n = sum(ex.map(work, slices))
+    t = time.perf_counter() - t0
+    return n / t / 1e6, dict(cores=threads, rows=len(rows), nvis=int(n), seconds=t,
+                             sample="%d of %d rows (every %d-th), all %d channels x %d pols; one degrid + one grid pass"
+                             % (len(rows), nrow_all, step, len(freq), d["npol"]))
+
+
+# --------------------------------------------------------------------------
+# arms
+# --------------------------------------------------------------------------
+def run_b200(args, w):
+    import torch
+    from yandasoft_b200 import build
+    from yandasoft_b200 import gridder as G
+    build.build()
+    G.load()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    d = gen_device(w)
+    nx = w["nx"]
+    cell = w["cell"] * ARCSEC
+    axes = G.Axes(cell, cell)
+    ps = parset_for(w, d["wmax"])
+    npol = d["npol"]
+    nvis = d["nrow"] * d["nchan"] * npol
+    acc = G.Accessor(d["uvw"], d["freq"], d["vis"], shape=(d["nrow"], d["nchan"], npol))
+    model_buf = torch.zeros_like(d["vis"])
+    acc_model = G.Accessor(d["uvw"], d["freq"], model_buf, shape=(d["nrow"], d["nchan"], npol))
+    gg = G.VisGridderFactory.make(ps)
+    gg.initialiseGrid(axes, (nx, nx, npol, 1))
+    gd = gg.clone()
+    img = model_image(w, d["sky"], npol)
+    gd.initialiseDegrid(axes, img)
+    t0 = time.perf_counter()
+    plan = gg.plan(acc)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
+    info = plan.info()
+    support = gg.support()[0]
+    stream = torch.cuda.ExternalStream(gg.stream_handle())
+
+    def step():
+        gd.degrid_plan(plan, acc_model)
+        gg.grid_plan(plan, acc)
+
+    for _ in range(args.warmup):
+        step()
+    gg.synchronize()
+    gd.synchronize()
+    k0 = gg.kernel_times()
+    k0d = gd.kernel_times()
+    launches0 = G.kernel_launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = G.kernel_launch_count() - launches0
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    k1 = gg.kernel_times()
+    k1d = gd.kernel_times()
+    ms_step = ms / args.steps
+    value = world * nvis / (ms_step / 1e3) / 1e6
+    kgrid_ms = (k1["kgrid_ms"] - k0["kgrid_ms"]) / max(1.0, k1["kgrid_calls"] - k0["kgrid_calls"])
+    kdeg_ms = (k1d["kdegrid_ms"] - k0d["kdegrid_ms"]) / max(1.0, k1d["kdegrid_calls"] - k0d["kdegrid_calls"])
+    nvalid_vis = info["nvalid"] * npol
+    taps = (2 * support + 1) ** 2
+    # algorithmic HBM bytes of one k_grid launch: read each on-grid sample's
+    # visibilities once, write the (padded-tile) scratch once.
+    hbm_peak, peak_kind = peaks()
+    alg_bytes = nvalid_vis * 8.0 + info["nvalid"] * (4 + 4 + 4) + 0.0
+    achieved_gbs = alg_bytes / (kgrid_ms / 1e3) / 1e9 if kgrid_ms > 0 else 0.0
+    flops = 8.0 * taps * nvalid_vis
+    fp32_peak_tflops = 148 * 128 * 2 * ((clk.summary().get("sm_mhz") or 1965.0) * 1e6) / 1e12
+    line = {
+        "metric": "grid+degrid Mvis/s on 1 B200 (plain tabulated CF)",
+        "value": round(value, 3), "unit": "Mvis/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64", "data": "synthetic (seeded; see bench.py workload())",
+        "config": {"workload": w["name"], "gridder": w["gridder"], "vis_samples": int(nvis),
+                   "rows": int(d["nrow"]), "channels": d["nchan"], "pols": npol, "grid": [nx, nx, npol, 1],
+                   "support": support, "taps_per_sample": taps, "oversample": w["oversample"],
+                   "tile": info["tile"], "work_items": info["nitems"], "on_grid_samples": int(info["nvalid"]),
+                   "l2": "inputs (%.1f GB of visibilities) larger than L2" % (nvis * 8 / 1e9),
+                   "step": "one degrid pass + one grid pass over all samples, inputs resident in HBM",
+                   "plan_build_s": round(t_plan, 3)},
+        "roofline": {"bound": "hbm", "kernel": "k_grid", "achieved": round(achieved_gbs, 2),
+                     "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved_gbs / hbm_peak, 4), "traffic": None,
+                     "kgrid_ms": round(kgrid_ms, 4), "kdegrid_ms": round(kdeg_ms, 4),
+                     "fp32": {"achieved_tflops": round(flops / (kgrid_ms / 1e3) / 1e12, 3) if kgrid_ms > 0 else 0,
+                              "peak_tflops_at_sampled_clock": round(fp32_peak_tflops, 2),
+                              "frac": round(flops / (kgrid_ms / 1e3) / 1e12 / fp32_peak_tflops, 4) if kgrid_ms > 0 else 0,
+                              "note": "8 flops per tap per sample; 148 SMs x 128 FP32 lanes x 2 at the sampled SM clock"}},
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    del plan, gg, gd, acc, acc_model, model_buf
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if not args.no_e2e:
+        line["e2e"] = e2e_b200(args, w, d, ps, axes, img)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, inf = cpu_baseline(w, d)
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
+                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2)}
+        except Exception as e:  # the baseline must not hide the GPU result
+            line["cpu_baseline"] = {"value": None, "error": repr(e)}
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def e2e_b200(args, w, d, ps, axes, img):
+    """The same step through the IVisGridder C-ABI calls with pinned host
+    buffers: initialiseDegrid, degrid (host cube in/out), initialiseGrid, grid,
+    finaliseGrid (image to host)."""
+    import torch
+    from yandasoft_b200 import gridder as G
+    npol, nchan, nrow = d["npol"], d["nchan"], d["nrow"]
+    vis_h = torch.empty(d["vis"].shape, dtype=d["vis"].dtype, pin_memory=True)
+    vis_h.copy_(d["vis"])
+    model_h = torch.zeros(d["vis"].shape, dtype=d["vis"].dtype, pin_memory=True)
+    uvw_h = torch.from_numpy(d["uvw_np"]).pin_memory()
+    freq_h = torch.from_numpy(d["freq_np"]).pin_memory()
+
+    vis_np = vis_h.numpy().view(np.complex64).reshape(-1)
+    cube = vis_np.reshape((nrow, nchan, npol), order="F")
+    mcube = model_h.numpy().view(np.complex64).reshape(-1).reshape((nrow, nchan, npol), order="F")
+    uvw_np = uvw_h.numpy()
+    freq_np = freq_h.numpy()
+    acc = G.Accessor(uvw_np, freq_np, cube)
+    accm = G.Accessor(uvw_np, freq_np, mcube)
+    gd = G.VisGridderFactory.make(ps)
+    gg = G.VisGridderFactory.make(ps)
+    nx = w["nx"]
+    out = np.zeros((nx, nx, npol, 1), dtype=np.float32, order="F")
+
+    def step():
+        gd.initialiseDegrid(axes, img)
+        gd.degrid(accm)
+        gg.initialiseGrid(axes, (nx, nx, npol, 1))
+        gg.grid(acc)
+        gg.finaliseGrid(out)
+
+    step()   # warm (CF generation, allocations)
+    torch.cuda.synchronize()
+    k = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    torch.cuda.synchronize()
+    t = (time.perf_counter() - t0) / k
+    nvis = nrow * nchan * npol
+    h2d = nvis * 8 * 2 + nrow * 24 * 2 + nchan * 8 * 2 + img.nbytes
+    d2h = nvis * 8 + out.nbytes
+    return {"value": round(nvis / t / 1e6, 3), "unit": "Mvis/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": round(t * 1e3, 2),
+            "path": "C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers"}
+
+
+def ctypes_ptr(t):
+    return t.data_ptr()
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    if torch.cuda.is_available():
+        d = gen_device(w)
+    else:
+        raise SystemExit("the reference arm needs the same synthetic generator (GPU)")
+    times = []
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, inf = cpu_baseline(w, d, target_s=8.0)
+        if s >= args.warmup:
+            vals.append(v)
+            times.append(inf["seconds"])
+    value = float(np.mean(vals))
+    line = {"metric": "grid+degrid Mvis/s on 1 B200 (plain tabulated CF)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mvis/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * float(np.mean(times)), 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
+            "config": {"workload": w["name"], "gridder": w["gridder"]},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
+                             "sample": inf["sample"]},
+            "e2e": {"value": round(value, 4), "unit": "Mvis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    w = workload(args.config, args.scale)
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

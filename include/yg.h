@@ -138,6 +138,10 @@ int yg_get_grid(const yg_gridder* g, float* out, int64_t capacity_complex, int32
 int yg_get_shape(const yg_gridder* g, int32_t* nx, int32_t* ny, int32_t* npol, int32_t* nchan);
 /* stats: samples/taps gridded, samples/taps degridded, ms grid, ms degrid, ms CF, CF planes built */
 int yg_get_stats(const yg_gridder* g, double* out8);
+/* device time of the tap kernels: k_grid ms, k_grid calls, k_degrid ms, k_degrid calls */
+int yg_get_kernel_times(const yg_gridder* g, double* out4);
+/* number of this library's own kernel launches so far (process-wide) */
+int64_t yg_kernel_launch_count(void);
 /* builds the convolution functions for the current axes without data
  * (SphFunc, WProject, WStack; AWProject builds from data). */
 int yg_build_cf(yg_gridder* g);
@@ -159,6 +163,8 @@ void yg_plan_destroy(yg_plan* plan);
 int yg_set_tile(yg_gridder* g, int32_t tile);      /* 0 = automatic */
 int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
 int yg_synchronize(yg_gridder* g);
+/* the cudaStream_t every kernel of this handle is launched on */
+int yg_get_stream(yg_gridder* g, void** stream);
 
 #ifdef __cplusplus
 }

@@ -253,6 +253,19 @@ int yg_get_shape(const yg_gridder* g, int32_t* nx, int32_t* ny, int32_t* npol, i
   });
 }
 
+int yg_get_kernel_times(const yg_gridder* g, double* out4) {
+  return guarded([&] {
+    if (!out4) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    const yg::Stats& s = G(g).stats();
+    out4[0] = s.kgrid_ms;
+    out4[1] = s.kgrid_calls;
+    out4[2] = s.kdegrid_ms;
+    out4[3] = s.kdegrid_calls;
+  });
+}
+
+int64_t yg_kernel_launch_count(void) { return yg::g_kernel_launches.load(); }
+
 int yg_get_stats(const yg_gridder* g, double* out8) {
   return guarded([&] {
     if (!out8) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
@@ -335,6 +348,15 @@ int yg_set_item_size(yg_gridder* g, int32_t vmax) {
   return guarded([&] {
     if (vmax < 1) throw yg::YgError{YG_ERR_ARG, "item size must be positive"};
     G(g).set_vmax(vmax);
+  });
+}
+
+int yg_get_stream(yg_gridder* g, void** stream) {
+  return guarded([&] {
+    if (!stream) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    yg::Gridder& x = G(g);
+    x.ensure_device();
+    *stream = (void*)x.stream();
   });
 }
 

@@ -60,6 +60,9 @@ CFView CFCacheDev::view() const {
   v.ncf = ncf;
   v.noffsets = noffsets;
   v.maxsize = maxsize;
+  v.varsup = 0;
+  for (int sz : h_size)
+    if (sz != 0 && sz != maxsize) v.varsup = 1;
   return v;
 }
 
@@ -70,6 +73,9 @@ int CFCacheDev::layout(const std::vector<int>& sizes, const std::vector<int2>& o
   long long tot = 0;
   maxsize = 0;
   for (int i = 0; i < ncf; ++i) {
+    // every plane starts on a 16-byte boundary (an even complex index) so
+    // that it can be bulk-copied into shared memory
+    tot = (tot + 1) & ~1ll;
     h_off[i] = tot;
     tot += (long long)sizes[i] * sizes[i];
     maxsize = std::max(maxsize, sizes[i]);
@@ -77,7 +83,9 @@ int CFCacheDev::layout(const std::vector<int>& sizes, const std::vector<int2>& o
   total = tot;
   h_offsets = offs;
   noffsets = (int)offs.size();
-  CF_TRY(data.ensure(std::max<long long>(tot, 1) * sizeof(float2)));
+  // slack so that a copy rounded up to 16 bytes never leaves the allocation
+  CF_TRY(data.ensure((std::max<long long>(tot, 1) + 2) * sizeof(float2)));
+  CF_TRY(cudaMemset(data.p, 0, (std::max<long long>(tot, 1) + 2) * sizeof(float2)));
   CF_TRY(off.ensure(std::max(ncf, 1) * sizeof(long long)));
   CF_TRY(size.ensure(std::max(ncf, 1) * sizeof(int)));
   CF_TRY(offsets.ensure(std::max(noffsets, 1) * sizeof(int2)));
@@ -102,7 +110,7 @@ int cf_build_sphfunc(CFCacheDev& cache, int support, int os, double alpha) {
   std::vector<int> sizes(os * os, cs);
   int e = cache.layout(sizes, {});
   if (e) return e;
-  std::vector<float2> h((size_t)os * os * cs * cs);
+  std::vector<float2> h(cache.total + 2, make_float2(0.f, 0.f));
   std::vector<float> bx(cs), by(cs);
   for (int fv = 0; fv < os; ++fv) {
     for (int fu = 0; fu < os; ++fu) {
@@ -113,7 +121,7 @@ int cf_build_sphfunc(CFCacheDev& cache, int support, int os, double alpha) {
         bx[i] = (float)(grdsf(nux) * std::pow(1.0 - nux * nux, alpha));
         by[i] = (float)(grdsf(nuy) * std::pow(1.0 - nuy * nuy, alpha));
       }
-      float2* c = h.data() + (size_t)plane * cs * cs;
+      float2* c = h.data() + cache.h_off[plane];
       // norm = float sum of |cf| over column-major order
       float norm = 0.f;
       for (int iy = 0; iy < cs; ++iy)

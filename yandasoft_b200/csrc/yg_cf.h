@@ -1,5 +1,6 @@
 // Convolution-function cache and its GPU builders.
 #pragma once
+#include <atomic>
 #include <vector>
 
 #include "yg_internal.h"
@@ -58,14 +59,16 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
 // gridding entry points (yg_gridding.cu)
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st);
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevError* err, cudaStream_t st);
+              DevBuf& scratch, DevError* err, cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
               int nchan_img, double* sumw, DevError* err, cudaStream_t st);
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st);
+                cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
-size_t grid_smem_bytes(int npol, int P);
-int grid_pols_per_pass(int npol, int P);
+size_t grid_smem_bytes(int npol, int P, int cfbuf);
+int grid_pols_per_pass(int npol, int P, int cfbuf);
+int grid_cf_buffer_bytes(int maxsize);
+extern std::atomic<long long> g_kernel_launches;
 
 }  // namespace yg

@@ -700,13 +700,17 @@ void Gridder::init_cf(const Chunk& dc) {
 // ---------------------------------------------------------------------------
 int Gridder::tile_for(int smax, int npol) const {
   if (tile_override_ > 0) return tile_override_;
-  // largest multiple of 8 whose padded tile fits ~110 KB of shared memory for
-  // the polarisations accumulated per pass (two CTAs per SM), else 220 KB
+  // largest multiple of 8 whose padded tile, with the two CF buffers, fits
+  // ~110 KB of shared memory for the polarisations accumulated per pass (two
+  // CTAs per SM), else 220 KB (one CTA per SM)
+  const int cfbuf = grid_cf_buffer_bytes(2 * smax + 1);
   const int budgets[2] = {110 * 1024, 220 * 1024};
   for (int b : budgets) {
     for (int npa : {npol, 2, 1}) {
       if (npa > npol || npol % npa) continue;
-      const double pmax = std::sqrt((double)(b - 4096) / (8.0 * npa));
+      const double rest = (double)b - 2.0 * cfbuf - 4096.0;
+      if (rest <= 0) continue;
+      const double pmax = std::sqrt(rest / (8.0 * npa));
       const int t = ((int)pmax - 2 * smax) / 8 * 8;
       if (t >= 32) return std::min(t, 256);
     }
@@ -799,8 +803,8 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
              "Check frequencies in the input file as the order of magnitude is likely to be wrong");
   }
   const std::vector<int> cmap = chan_map(freqs.data(), dc.nchan);
-  cuda_check(chanmap_d_.ensure(std::max(1, dc.nchan) * sizeof(int)), "alloc");
-  cuda_check(cudaMemcpyAsync(chanmap_d_.p, cmap.data(), dc.nchan * sizeof(int), cudaMemcpyHostToDevice, stream_), "up");
+  cuda_check(pl.chanmap.ensure(std::max(1, dc.nchan) * sizeof(int)), "alloc");
+  cuda_check(cudaMemcpyAsync(pl.chanmap.p, cmap.data(), dc.nchan * sizeof(int), cudaMemcpyHostToDevice, stream_), "up");
   std::vector<uint8_t> rows = psf_rows(dc);
   const uint8_t* row_ok = nullptr;
   if (!rows.empty()) {
@@ -809,8 +813,14 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
     row_ok = rowok_d_.as<uint8_t>();
   }
   BinArgs a;
-  fill_bin_args(a, dc, chanmap_d_.as<int>(), row_ok);
-  rc_check(plan_build(pl, a, vmax_, err_.as<DevError>(), stream_), "binning");
+  fill_bin_args(a, dc, pl.chanmap.as<int>(), row_ok);
+  // samples per work item: enough items for ~8 per SM, never below 512
+  int vmax = vmax_;
+  if (vmax <= 0) {
+    const long long n = dc.nrow * (long long)dc.nchan;
+    vmax = (int)std::min<long long>(1 << 20, std::max<long long>(512, n / (148 * 8)));
+  }
+  rc_check(plan_build(pl, a, vmax, err_.as<DevError>(), stream_), "binning");
   check_error();
 }
 
@@ -845,6 +855,9 @@ void Gridder::grid(const Chunk& c) {
 }
 
 void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
+  throw_if(!grids_.p || nx_ == 0, YG_ERR_STATE, "initialiseGrid must be called before grid");
+  if (kind_ != Kind::AWProject) build_cf();
+  throw_if(!cf_built_, YG_ERR_STATE, "convolution functions are not built");
   const float* mfs = nullptr;
   if (mfs_) {
     const std::vector<double> f = host_freqs(dc);
@@ -858,22 +871,32 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
     mfs = mfs_d_.as<float>();
   }
   VisArgs v = vis_args(dc, mfs, psf_);
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0, e1, k0, k1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  cudaEventCreate(&k0);
+  cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  rc_check(plan_sumw(pl, v, chanmap_d_.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_, sumw_.as<double>(),
+  rc_check(plan_sumw(pl, v, pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_, sumw_.as<double>(),
                      err_.as<DevError>(), stream_),
            "sum of weights");
-  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, scratch_, err_.as<DevError>(), stream_),
+  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, scratch_, err_.as<DevError>(), stream_,
+                     k0, k1),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
   cudaEventRecord(e1, stream_);
   check_error();
-  float ms = 0;
+  float ms = 0, kms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
+  if (pl.nitems > 0 && cudaEventElapsedTime(&kms, k0, k1) == cudaSuccess) {
+    stats_.kgrid_ms += kms;
+    stats_.kgrid_calls += 1;
+  }
+  cudaGetLastError();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaEventDestroy(k0);
+  cudaEventDestroy(k1);
   stats_.time_grid_ms += ms;
   stats_.samples_gridded += (double)pl.nvalid * dc.npol;
   const double w = 2.0 * cf_.support + 1.0;
@@ -899,6 +922,9 @@ void Gridder::degrid(Chunk& c) {
 }
 
 void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
+  throw_if(!grids_.p || nx_ == 0, YG_ERR_STATE, "initialiseDegrid must be called before degrid");
+  if (kind_ != Kind::AWProject) build_cf();
+  throw_if(!cf_built_, YG_ERR_STATE, "convolution functions are not built");
   const float* mfs = nullptr;
   if (mfs_) {
     const std::vector<double> f = host_freqs(dc);
@@ -912,19 +938,28 @@ void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
     mfs = mfs_d_.as<float>();
   }
   VisArgs v = vis_args(dc, mfs, false);
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0, e1, k0, k1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  cudaEventCreate(&k0);
+  cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, chanmap_d_.as<int>(), tmpvals_,
-                       carry_.as<float2>(), err_.as<DevError>(), stream_),
+  rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
+                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1),
            "degridding");
   cudaEventRecord(e1, stream_);
   check_error();
-  float ms = 0;
+  float ms = 0, kms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
+  if (pl.nitems > 0 && cudaEventElapsedTime(&kms, k0, k1) == cudaSuccess) {
+    stats_.kdegrid_ms += kms;
+    stats_.kdegrid_calls += 1;
+  }
+  cudaGetLastError();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaEventDestroy(k0);
+  cudaEventDestroy(k1);
   stats_.time_degrid_ms += ms;
   stats_.samples_degridded += (double)pl.nvalid * dc.npol;
   const double w = 2.0 * cf_.support + 1.0;

@@ -64,6 +64,8 @@ struct Stats {
   double samples_degridded = 0, taps_degridded = 0;
   double time_grid_ms = 0, time_degrid_ms = 0, time_cf_ms = 0;
   double cf_generations = 0;
+  double kgrid_ms = 0, kdegrid_ms = 0;   // k_grid / k_degrid only (CUDA events)
+  double kgrid_calls = 0, kdegrid_calls = 0;
 };
 
 class Gridder {
@@ -179,7 +181,7 @@ class Gridder {
   int rep_feed_ = 0;
   double rep_pointing_[2] = {0, 0};
   int tile_override_ = 0;
-  int vmax_ = 1024;
+  int vmax_ = 0;   // samples per work item, 0 = automatic
 
   CFCacheDev cf_;
   bool cf_built_ = false;

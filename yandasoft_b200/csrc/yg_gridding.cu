@@ -25,11 +25,16 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "yg_internal.h"
 
 namespace yg {
+
+// number of this library's own kernel launches (cub's are not counted)
+std::atomic<long long> g_kernel_launches{0};
+#define YG_COUNT_LAUNCH() g_kernel_launches.fetch_add(1, std::memory_order_relaxed)
 
 
 __device__ __forceinline__ unsigned int morton2(unsigned int x, unsigned int y) {
@@ -236,6 +241,7 @@ __global__ void k_sumw(VisArgs v, const unsigned char* __restrict__ status, cons
 struct GridKArgs {
   const int4* items;
   const unsigned int* val;   // sample ids, sorted
+  const int* runend;         // per sorted index at a run start: end of its run
   const unsigned int* pos;   // iu | iv << 16, unsorted (by sample id)
   const int* cfi;            // unsorted
   VisArgs v;
@@ -244,6 +250,7 @@ struct GridKArgs {
   long long ntiles;
   int smax;                  // Smax of the plan
   int P;                     // T + 2 Smax
+  int cfbuf;                 // bytes of one shared-memory CF buffer
   float2* scratch;           // [item][npol][P][P]
   int pol0;                  // first polarisation of this pass
   int npol_total;            // polarisations of the visibility cube
@@ -252,132 +259,226 @@ struct GridKArgs {
 
 constexpr int kGridThreads = 256;
 constexpr int kBatch = 64;
+constexpr long long kWaitLimit = 1ll << 22;   // bounded mbarrier waits
 
 struct VisRec {
-  int px0, py0;      // footprint origin inside the padded tile
+  int cb;            // footprint origin cell (px0 + P py0) in the padded tile
   int mx, my;        // px0 mod W, py0 mod W
   int w;             // 2S+1 of this CF
-  int pad_;
-  long long cfoff;   // CF offset (elements)
 };
 
-template <int NPOL, int MAXSLOTS>
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// one-dimensional TMA bulk copy global -> shared, completion on the mbarrier
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// bounded wait; false when the limit was reached
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
+  for (long long i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+
+__host__ __device__ __forceinline__ unsigned cf_bytes(int w) { return (unsigned)(((w * w * 8) + 15) & ~15); }
+
+// Gridding of one work item.  CF planes are shared by runs of consecutive
+// samples (the sort key orders samples by CF inside a tile); each run's plane
+// is brought into shared memory by a TMA bulk copy one run ahead.
+template <int NPOL, int MAXSLOTS, bool VARSUP>
 __global__ void __launch_bounds__(kGridThreads) k_grid(GridKArgs a) {
-  extern __shared__ float4 smem_raw[];
-  float2* acc_s = reinterpret_cast<float2*>(smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int P = a.P;
   const int P2 = P * P;
-  VisRec* recs = reinterpret_cast<VisRec*>(acc_s + (size_t)NPOL * P2);
+  float2* acc_s = reinterpret_cast<float2*>(smem_raw);
+  unsigned char* cfb = smem_raw + (size_t)NPOL * P2 * sizeof(float2);
+  cfb = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(cfb) + 127) & ~(size_t)127);
+  float2* cfs[2] = {reinterpret_cast<float2*>(cfb), reinterpret_cast<float2*>(cfb + a.cfbuf)};
+  VisRec* recs = reinterpret_cast<VisRec*>(cfb + 2 * (size_t)a.cfbuf);
   float2* vals = reinterpret_cast<float2*>(recs + kBatch);
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(vals + kBatch * NPOL);
+  __shared__ int s_abort;
 
   const int4 it = a.items[blockIdx.x];
-  const long long tile_id = it.x;
-  const long long t = tile_id % a.ntiles;
+  const long long t = (long long)it.x % a.ntiles;
   const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
   const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
   const int W = 2 * a.smax + 1;
   const int W2 = W * W;
 
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
   for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+
+  auto issue = [&](int start, int buf) {
+    const unsigned s = a.val[start];
+    const int c = a.cfi[s];
+    const unsigned bytes = cf_bytes(a.cf.size[c]);
+    mbar_expect_tx(&bars[buf], bytes);
+    bulk_g2s(cfs[buf], a.cf.data + a.cf.off[c], bytes, &bars[buf]);
+  };
+  // end of the run containing sorted index j, inside this item (always > j)
+  auto run_end = [&](int j) { return max(j + 1, min(a.runend[j], it.z)); };
+  if (threadIdx.x == 0) {
+    issue(it.y, 0);
+    const int e0 = run_end(it.y);
+    if (e0 < it.z) issue(e0, 1);
+  }
 
   int rx[MAXSLOTS], ry[MAXSLOTS], cur[MAXSLOTS];
   float2 acc[MAXSLOTS][NPOL];
 #pragma unroll
   for (int q = 0; q < MAXSLOTS; ++q) {
-    const int k = q * blockDim.x + threadIdx.x;
+    const int k = q * kGridThreads + threadIdx.x;
     rx[q] = k < W2 ? k % W : -1;
     ry[q] = k < W2 ? k / W : -1;
     cur[q] = -1;
 #pragma unroll
     for (int p = 0; p < NPOL; ++p) acc[q][p] = make_float2(0.f, 0.f);
   }
-  __syncthreads();
 
   const long long n = a.v.nrow * (long long)a.v.nchan;
-  for (int base = it.y; base < it.z; base += kBatch) {
-    const int nb = min(kBatch, it.z - base);
-    // stage visibility records
-    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-      const unsigned int s = a.val[base + j];
-      const unsigned int ps = a.pos[s];
-      const int c = a.cfi[s];
-      const int w = a.cf.size[c];
-      const int sup = (w - 1) / 2;
-      VisRec r;
-      r.px0 = (int)(ps & 0xffffu) - sup - X0;
-      r.py0 = (int)(ps >> 16) - sup - Y0;
-      r.mx = r.px0 % W;
-      r.my = r.py0 % W;
-      r.w = w;
-      r.pad_ = 0;
-      r.cfoff = a.cf.off[c];
-      recs[j] = r;
-      const long long row = s % a.v.nrow;
-      const int chan = (int)(s / a.v.nrow);
-      float pr, pi;
-      phasor_of(a.v, row, chan, &pr, &pi);
-      const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
-      const bool use = !(a.v.psf && a.v.psf_ok && !a.v.psf_ok[row]);
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        const int pp = a.pol0 + p;
-        const float nre = a.v.noise ? a.v.noise[s + n * pp].x : 1.f;
-        const float wt = noise_weight(nre);
-        float2 o;
-        if (a.v.psf) {
-          o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
-          o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
-        } else {
-          const float2 vv = a.v.vis[s + n * pp];
-          const float vr = vv.x, vi = -vv.y;
-          float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
-          float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
-          rr = __fmul_rn(__fmul_rn(rr, wt), m);
-          ri = __fmul_rn(__fmul_rn(ri, wt), m);
-          o = make_float2(rr, ri);
-        }
-        if (!use) o = make_float2(0.f, 0.f);
-        vals[j * NPOL + p] = o;
-      }
+  unsigned phase[2] = {0u, 0u};
+  int b = 0;
+  for (int j = it.y; j < it.z;) {
+    const int e = run_end(j);
+    if (!mbar_wait(&bars[b], phase[b])) {
+      if (threadIdx.x == 0) raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+      s_abort = 1;
     }
+    phase[b] ^= 1u;
     __syncthreads();
-    for (int j = 0; j < nb; ++j) {
-      const VisRec r = recs[j];
-      float2 vv[NPOL];
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) vv[p] = vals[j * NPOL + p];
-      const float2* __restrict__ cfp = a.cf.data + r.cfoff;
-#pragma unroll
-      for (int q = 0; q < MAXSLOTS; ++q) {
-        if (rx[q] < 0) continue;
-        int jx = rx[q] - r.mx;
-        jx += (jx < 0) ? W : 0;
-        int jy = ry[q] - r.my;
-        jy += (jy < 0) ? W : 0;
-        if (jx >= r.w || jy >= r.w) continue;
-        const int cell = (r.px0 + jx) + P * (r.py0 + jy);
-        const float2 c = __ldg(cfp + jx + r.w * jy);
-        if (cell != cur[q]) {
-          if (cur[q] >= 0) {
-#pragma unroll
-            for (int p = 0; p < NPOL; ++p) {
-              float2 g = acc_s[p * P2 + cur[q]];
-              g.x += acc[q][p].x;
-              g.y += acc[q][p].y;
-              acc_s[p * P2 + cur[q]] = g;
-              acc[q][p] = make_float2(0.f, 0.f);
-            }
-          }
-          cur[q] = cell;
-        }
+    if (s_abort) break;
+    const float2* __restrict__ cf_s = cfs[b];
+    for (int base = j; base < e; base += kBatch) {
+      const int nb = min(kBatch, e - base);
+      for (int jj = threadIdx.x; jj < nb; jj += blockDim.x) {
+        const unsigned int s = a.val[base + jj];
+        const unsigned int ps = a.pos[s];
+        const int c = a.cfi[s];
+        const int w = a.cf.size[c];
+        const int sup = (w - 1) / 2;
+        const int px0 = (int)(ps & 0xffffu) - sup - X0;
+        const int py0 = (int)(ps >> 16) - sup - Y0;
+        VisRec r;
+        r.cb = px0 + P * py0;
+        r.mx = px0 % W;
+        r.my = py0 % W;
+        r.w = w;
+        recs[jj] = r;
+        const long long row = s % a.v.nrow;
+        const int chan = (int)(s / a.v.nrow);
+        float pr, pi;
+        phasor_of(a.v, row, chan, &pr, &pi);
+        const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) {
-          acc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, acc[q][p].x));
-          acc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, acc[q][p].y));
+          const int pp = a.pol0 + p;
+          const float nre = a.v.noise ? a.v.noise[s + n * pp].x : 1.f;
+          const float wt = noise_weight(nre);
+          float2 o;
+          if (a.v.psf) {
+            o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
+            o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
+          } else {
+            const float2 vv = a.v.vis[s + n * pp];
+            const float vr = vv.x, vi = -vv.y;
+            float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+            float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+            rr = __fmul_rn(__fmul_rn(rr, wt), m);
+            ri = __fmul_rn(__fmul_rn(ri, wt), m);
+            o = make_float2(rr, ri);
+          }
+          vals[jj * NPOL + p] = o;
         }
       }
+      __syncthreads();
+      for (int jj = 0; jj < nb; ++jj) {
+        const VisRec r = recs[jj];
+        float2 vv[NPOL];
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) vv[p] = vals[jj * NPOL + p];
+#pragma unroll
+        for (int q = 0; q < MAXSLOTS; ++q) {
+          if (rx[q] < 0) continue;
+          int jx = rx[q] - r.mx;
+          jx += (jx < 0) ? W : 0;
+          int jy = ry[q] - r.my;
+          jy += (jy < 0) ? W : 0;
+          if (VARSUP && (jx >= r.w || jy >= r.w)) continue;
+          const int cell = r.cb + jx + P * jy;
+          const float2 c = cf_s[jx + r.w * jy];
+          if (cell != cur[q]) {
+            if (cur[q] >= 0) {
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) {
+                float2 g = acc_s[p * P2 + cur[q]];
+                g.x += acc[q][p].x;
+                g.y += acc[q][p].y;
+                acc_s[p * P2 + cur[q]] = g;
+                acc[q][p] = make_float2(0.f, 0.f);
+              }
+            }
+            cur[q] = cell;
+          }
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            acc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, acc[q][p].x));
+            acc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, acc[q][p].y));
+          }
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    // buffer b is free: bring the run after the next one into it
+    if (threadIdx.x == 0 && e < it.z) {
+      const int e2 = run_end(e);
+      if (e2 < it.z) {
+        fence_proxy_async_smem();
+        issue(e2, b);
+      }
+    }
+    j = e;
+    b ^= 1;
+  }
+  if (s_abort) {
+    // let any copy still in flight land before the CTA's shared memory goes away
+    if (threadIdx.x == 0) {
+      mbar_wait(&bars[0], phase[0]);
+      mbar_wait(&bars[1], phase[1]);
+    }
+    return;
   }
 #pragma unroll
   for (int q = 0; q < MAXSLOTS; ++q) {
@@ -394,6 +495,23 @@ __global__ void __launch_bounds__(kGridThreads) k_grid(GridKArgs a) {
   __syncthreads();
   float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
   for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) out[i] = acc_s[i];
+}
+
+// Run ends of the sorted list (a run = consecutive samples of one tile with
+// the same CF index).  rev[j], j = nvalid-1-i, holds i+1 when a new run starts
+// at i+1 (or i+1 == nvalid) and INT_MAX otherwise; a prefix-min over rev gives
+// for every i the first run start after it.
+__global__ void k_run_marks(const unsigned long long* __restrict__ key, long long nvalid, int mbits,
+                            int* __restrict__ rev) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
+    const bool brk = (i + 1 == nvalid) || ((key[i + 1] >> mbits) != (key[i] >> mbits));
+    rev[nvalid - 1 - i] = brk ? (int)(i + 1) : 0x7fffffff;
+  }
+}
+
+__global__ void k_run_unreverse(const int* __restrict__ revmin, long long nvalid, int* __restrict__ runend) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x)
+    runend[i] = revmin[nvalid - 1 - i];
 }
 
 // ---------------------------------------------------------------------------
@@ -493,20 +611,28 @@ struct DegridKArgs {
 
 constexpr int kDegridThreads = 256;
 
+// One warp per visibility.  Lanes walk the taps with a shared table of tap ->
+// cell offsets and keep four independent partial sums per polarisation so
+// that loads of later taps overlap the FMAs of earlier ones; the partial sums
+// are combined with warp shuffles.
 template <int NPOL>
 __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int P = a.P, P2 = P * P;
+  const int W = 2 * a.smax + 1, W2 = W * W;
   float2* g_s = reinterpret_cast<float2*>(smem_raw);
+  int* tab = reinterpret_cast<int*>(smem_raw + (a.smem_grid ? (size_t)NPOL * P2 * sizeof(float2) : 0));
   const int4 it = a.items[blockIdx.x];
   const long long tile_id = it.x;
   const long long gc = tile_id / a.ntiles;
   const long long t = tile_id % a.ntiles;
   const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
   const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
-  const int P = a.P, P2 = P * P;
   const int gind = (int)(gc / a.nchan_img), ichan = (int)(gc % a.nchan_img);
   const long long plane_cells = (long long)a.nx * a.ny;
   const float2* gbase = a.grid + (size_t)gind * plane_cells * NPOL * a.nchan_img + plane_cells * ((size_t)NPOL * ichan);
+  const int stride = a.smem_grid ? P : a.nx;
+  for (int i = threadIdx.x; i < W2; i += blockDim.x) tab[i] = (i % W) + stride * (i / W);
   if (a.smem_grid) {
     for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
       const int px = i % P, py = (i / P) % P, p = i / P2;
@@ -515,49 +641,74 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
       if (x >= 0 && y >= 0 && x < a.nx && y < a.ny) g = gbase[plane_cells * p + x + (size_t)a.nx * y];
       g_s[i] = g;
     }
-    __syncthreads();
   }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
-  const long long n = a.v.nrow * (long long)a.v.nchan;
+  const float2* src = a.smem_grid ? g_s : gbase;
+  const long long pstride = a.smem_grid ? P2 : plane_cells;
   for (int i = it.y + warp; i < it.z; i += nwarps) {
     const unsigned int s = a.val[i];
     const unsigned int ps = a.pos[s];
     const int c = a.cfi[s];
     const int w = a.cf.size[c];
     const int sup = (w - 1) / 2;
-    const int px0 = (int)(ps & 0xffffu) - sup - X0;
-    const int py0 = (int)(ps >> 16) - sup - Y0;
+    const int px0 = (int)(ps & 0xffffu) - sup;
+    const int py0 = (int)(ps >> 16) - sup;
+    const long long origin = a.smem_grid ? (long long)(px0 - X0) + (long long)P * (py0 - Y0)
+                                         : (long long)px0 + (long long)a.nx * py0;
     const float2* __restrict__ cfp = a.cf.data + a.cf.off[c];
-    float re[NPOL], im[NPOL];
+    float re[4][NPOL], im[4][NPOL];
 #pragma unroll
-    for (int p = 0; p < NPOL; ++p) { re[p] = 0.f; im[p] = 0.f; }
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) { re[u][p] = 0.f; im[u][p] = 0.f; }
     const int ntaps = w * w;
-    int jx = lane % w, jy = lane / w;
-    for (int tp = lane; tp < ntaps; tp += 32) {
-      const float2 cv = __ldg(cfp + tp);
+    if (w == W) {
+      for (int tp = lane; tp < ntaps; tp += 128) {
+        int o[4];
+        float2 cv[4];
 #pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        float2 g;
-        if (a.smem_grid) {
-          g = g_s[p * P2 + (px0 + jx) + P * (py0 + jy)];
-        } else {
-          g = __ldg(gbase + plane_cells * p + (X0 + px0 + jx) + (size_t)a.nx * (Y0 + py0 + jy));
+        for (int u = 0; u < 4; ++u) {
+          const int tu = tp + 32 * u;
+          o[u] = tu < ntaps ? tab[tu] : 0;
+          cv[u] = tu < ntaps ? __ldg(cfp + tu) : make_float2(0.f, 0.f);
         }
-        re[p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[p]));
-        im[p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[p]));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            const float2 g = src[pstride * p + origin + o[u]];
+            re[u][p] = fmaf(cv[u].x, g.x, fmaf(cv[u].y, g.y, re[u][p]));
+            im[u][p] = fmaf(cv[u].y, g.x, fmaf(-cv[u].x, g.y, im[u][p]));
+          }
+        }
       }
-      jx += 32;
-      while (jx >= w) { jx -= w; ++jy; }
+    } else {
+      // plane with its own (smaller) support
+      for (int tp = lane; tp < ntaps; tp += 32) {
+        const int jx = tp % w, jy = tp / w;
+        const float2 cv = __ldg(cfp + tp);
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          const float2 g = src[pstride * p + origin + jx + (long long)stride * jy];
+          re[0][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[0][p]));
+          im[0][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[0][p]));
+        }
+      }
     }
 #pragma unroll
     for (int p = 0; p < NPOL; ++p) {
+      float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
+      float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        re[p] += __shfl_xor_sync(0xffffffffu, re[p], o);
-        im[p] += __shfl_xor_sync(0xffffffffu, im[p], o);
+      for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
       }
+      re[0][p] = sr;
+      im[0][p] = si;
     }
     if (lane == 0) {
       const long long row = s % a.v.nrow;
@@ -567,7 +718,7 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
       const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
 #pragma unroll
       for (int p = 0; p < NPOL; ++p) {
-        float cr = re[p], ci = im[p];
+        float cr = re[0][p], ci = im[0][p];
         if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
         const float orr = __fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi));
         const float oi = __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr));
@@ -575,7 +726,6 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
       }
     }
   }
-  (void)n;
 }
 
 // prev[o] = o when sample (row, chan) with o = row * nchan + chan is on-grid,
@@ -690,6 +840,7 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   k_bin<<<grid_dim(n, 256), 256, 0, st>>>(a, pl.key.as<unsigned long long>(), pl.val.as<unsigned int>(),
                                           pl.pos.as<unsigned int>(), pl.cfi.as<int>(),
                                           pl.status.as<unsigned char>(), err);
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   // radix sort over the bits that keys use (the invalid key is one past the
   // largest valid key, so it sorts last)
@@ -721,7 +872,9 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   k_tile_bounds<<<grid_dim(n, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), n, a.mbits, a.cf.ncf,
                                                   a.invalid_key, pl.tstart.as<int>(), pl.tend.as<int>(),
                                                   pl.nvalid_d.as<long long>());
+  YG_COUNT_LAUNCH();
   k_count_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), nt, vmax, pl.nit.as<int>());
+  YG_COUNT_LAUNCH();
   size_t tmp2 = 0;
   YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
   if (tmp2 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp2));
@@ -737,50 +890,73 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   YG_CUDA_TRY(pl.items.ensure((size_t)std::max(1, pl.nitems) * sizeof(int4)));
   k_fill_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), pl.nit.as<int>(),
                                                   pl.itembase.as<int>(), nt, vmax, pl.items.as<int4>());
+  YG_COUNT_LAUNCH();
+  YG_CUDA_TRY(pl.runend.ensure((size_t)std::max(1ll, pl.nvalid) * 4));
+  if (pl.nvalid > 0) {
+    // scratch for the marks: the (now unused) alternate key buffer
+    int* rev = pl.key_alt.as<int>();
+    int* revmin = rev + pl.nvalid;
+    k_run_marks<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), pl.nvalid, a.mbits, rev);
+    YG_COUNT_LAUNCH();
+    size_t tmp3 = 0;
+    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp3, rev, revmin, cub::Min(), (int)pl.nvalid, st));
+    if (tmp3 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp3));
+    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp3, rev, revmin, cub::Min(), (int)pl.nvalid, st));
+    k_run_unreverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(revmin, pl.nvalid, pl.runend.as<int>());
+    YG_COUNT_LAUNCH();
+  }
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
 
 static int max_slots_for(int W, int threads) { return (W * W + threads - 1) / threads; }
 
-template <int NPOL>
-static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, int slots, cudaStream_t st) {
-  if (slots <= 4) {
-    auto k = k_grid<NPOL, 4>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<nitems, kGridThreads, smem, st>>>(g);
-  } else if (slots <= 8) {
-    auto k = k_grid<NPOL, 8>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<nitems, kGridThreads, smem, st>>>(g);
-  } else if (slots <= 16) {
-    auto k = k_grid<NPOL, 16>;
+template <int NPOL, int MAXSLOTS>
+static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, size_t smem, bool varsup, cudaStream_t st) {
+  if (varsup) {
+    auto k = k_grid<NPOL, MAXSLOTS, true>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<nitems, kGridThreads, smem, st>>>(g);
   } else {
-    return cudaErrorInvalidConfiguration;
+    auto k = k_grid<NPOL, MAXSLOTS, false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<nitems, kGridThreads, smem, st>>>(g);
   }
+  YG_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
-size_t grid_smem_bytes(int npol, int P) {
-  return (size_t)npol * P * P * sizeof(float2) + kBatch * sizeof(VisRec) + (size_t)kBatch * npol * sizeof(float2);
+template <int NPOL>
+static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, int slots, bool varsup,
+                                  cudaStream_t st) {
+  if (slots <= 4) return launch_grid_ms<NPOL, 4>(g, nitems, smem, varsup, st);
+  if (slots <= 8) return launch_grid_ms<NPOL, 8>(g, nitems, smem, varsup, st);
+  if (slots <= 16) return launch_grid_ms<NPOL, 16>(g, nitems, smem, varsup, st);
+  return cudaErrorInvalidConfiguration;
+}
+
+// bytes of one shared-memory CF buffer for CFs of at most maxsize^2 taps
+int grid_cf_buffer_bytes(int maxsize) { return (int)((cf_bytes(maxsize) + 127u) & ~127u); }
+
+size_t grid_smem_bytes(int npol, int P, int cfbuf) {
+  return (size_t)npol * P * P * sizeof(float2) + 128 + 2 * (size_t)cfbuf + kBatch * sizeof(VisRec) +
+         (size_t)kBatch * npol * sizeof(float2) + 2 * sizeof(unsigned long long);
 }
 
 // Polarisations accumulated together in one k_grid pass: the most that fit
 // the shared-memory budget.
-int grid_pols_per_pass(int npol, int P) {
+int grid_pols_per_pass(int npol, int P, int cfbuf) {
   const int cands[3] = {4, 2, 1};
   for (int c : cands) {
     if (c > npol || npol % c) continue;
-    if (grid_smem_bytes(c, P) <= 227 * 1024) return c;
+    if (grid_smem_bytes(c, P, cfbuf) <= 227 * 1024) return c;
   }
   return 0;
 }
 
 // Grids the samples of a plan onto `grid` (ngrid planes of (nx, ny, npol, nchan_img)).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevError* err, cudaStream_t st) {
+              DevBuf& scratch, DevError* err, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
   if (pl.nitems == 0) return YG_OK;
   const int P = pl.pad;
   const int W = 2 * pl.smax + 1;
@@ -790,6 +966,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   GridKArgs g;
   g.items = pl.items.as<int4>();
   g.val = pl.val.as<unsigned int>();
+  g.runend = pl.runend.as<int>();
   g.pos = pl.pos.as<unsigned int>();
   g.cfi = pl.cfi.as<int>();
   g.v = v;
@@ -799,23 +976,26 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.ntiles = (long long)pl.ntx * pl.nty;
   g.smax = pl.smax;
   g.P = P;
+  g.cfbuf = grid_cf_buffer_bytes(cf.maxsize);
   g.scratch = scratch.as<float2>();
   g.npol_total = v.npol;
   g.err = err;
-  const int npa = grid_pols_per_pass(v.npol, P);
+  const int npa = grid_pols_per_pass(v.npol, P, g.cfbuf);
   if (npa == 0) return YG_ERR_UNSUPPORTED;
-  const size_t smem = grid_smem_bytes(npa, P);
+  const size_t smem = grid_smem_bytes(npa, P, g.cfbuf);
+  if (ev0) cudaEventRecord(ev0, st);
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
     cudaError_t e;
     switch (npa) {
-      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, slots, st); break;
-      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, slots, st); break;
-      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, slots, st); break;
+      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
+      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
+      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
       default: return YG_ERR_UNSUPPORTED;
     }
     if (e != cudaSuccess) return YG_ERR_CUDA;
   }
+  if (ev1) cudaEventRecord(ev1, st);
   HaloArgs h;
   h.item_base = pl.itembase.as<int>();
   h.nit = pl.nit.as<int>();
@@ -834,6 +1014,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   const long long nblocks = pl.ntiles_total;
   if (nblocks > 0x7fffffffll) return YG_ERR_UNSUPPORTED;
   k_halo_sum<<<(unsigned)nblocks, 256, 0, st>>>(h);
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
@@ -843,6 +1024,7 @@ int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int
   if (pl.nsamples == 0) return YG_OK;
   k_sumw<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, pl.status.as<unsigned char>(), pl.cfi.as<int>(), chan_map,
                                                      os, track_per_os, nrows_sumw, nchan_img, sumw, err);
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
@@ -850,7 +1032,7 @@ int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int
 // Degrids the samples of a plan from `grid` and adds the result into vis.
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st) {
+                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
@@ -873,32 +1055,40 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     d.smax = pl.smax;
     d.P = pl.pad;
     d.out = tmp_vals.as<float2>();
-    size_t smem = (size_t)v.npol * pl.pad * pl.pad * sizeof(float2);
+    const int W = 2 * pl.smax + 1;
+    const size_t tab_bytes = (size_t)W * W * sizeof(int);
+    size_t smem = (size_t)v.npol * pl.pad * pl.pad * sizeof(float2) + tab_bytes;
     d.smem_grid = smem <= 200 * 1024 ? 1 : 0;
-    if (!d.smem_grid) smem = 0;
+    if (!d.smem_grid) smem = tab_bytes;
+    if (smem > 227 * 1024) return YG_ERR_UNSUPPORTED;
     cudaError_t e = cudaSuccess;
+    if (ev0) cudaEventRecord(ev0, st);
     switch (v.npol) {
       case 1: {
         auto k = k_degrid<1>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        YG_COUNT_LAUNCH();
         break;
       }
       case 2: {
         auto k = k_degrid<2>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        YG_COUNT_LAUNCH();
         break;
       }
       case 4: {
         auto k = k_degrid<4>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        YG_COUNT_LAUNCH();
         break;
       }
       default:
         return YG_ERR_UNSUPPORTED;
     }
+    if (ev1) cudaEventRecord(ev1, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return YG_ERR_CUDA;
   }
@@ -907,13 +1097,16 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
   int* marks = pl.order_prev.as<int>();
   int* prev = marks + n;
   k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 3, marks);
+  YG_COUNT_LAUNCH();
   size_t tmp = 0;
   YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
   YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
   YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
   k_degrid_writeback<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), prev, tmp_vals.as<float2>(),
                                                        carry, pl.nrow, pl.nchan, v.npol, vis_out);
+  YG_COUNT_LAUNCH();
   k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, tmp_vals.as<float2>(), 0, carry);
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
@@ -927,11 +1120,13 @@ int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st) 
   int* marks = pl.order_prev.as<int>();
   int* prev = marks + n;
   k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 1, marks);
+  YG_COUNT_LAUNCH();
   size_t tmp = 0;
   YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
   YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
   YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
   k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, v.vis, 1, carry);
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }

@@ -50,6 +50,7 @@ struct CFView {
   int ncf = 0;
   int noffsets = 0;
   int maxsize = 0;                 // max 2S+1 over the cache
+  int varsup = 0;                  // 1 when CF sizes differ (variable support)
 };
 
 // How a (row, chan, feed) sample maps to a CF plane and a grid.
@@ -100,6 +101,8 @@ struct Plan {
   DevBuf key, key_alt, val, val_alt, pos, cfi, status;
   DevBuf tstart, tend, nit, itembase, items, nvalid_d, sort_tmp;
   DevBuf order_prev;            // degrid stale-value scan
+  DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
+  DevBuf runend;                // end of each run of equal (tile, CF) samples, at its start
   double taps = 0;              // sum of (2S+1)^2 over valid samples (per pol)
 };
 

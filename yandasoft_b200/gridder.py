@@ -35,7 +35,7 @@ EXPORTS = [
     "yg_init_vis_weights_mfs", "yg_is_model_empty", "yg_get_support", "yg_get_cf", "yg_get_cf_offsets",
     "yg_get_sum_weights", "yg_get_grid", "yg_get_shape", "yg_get_stats", "yg_build_cf", "yg_plan_create",
     "yg_plan_grid", "yg_plan_degrid", "yg_plan_info", "yg_plan_samples", "yg_plan_destroy", "yg_set_tile", "yg_set_item_size",
-    "yg_synchronize",
+    "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
 ]
 
 
@@ -99,6 +99,10 @@ def load(path: str | None = None):
     L.yg_set_tile.argtypes = [P, I32]
     L.yg_set_item_size.argtypes = [P, I32]
     L.yg_synchronize.argtypes = [P]
+    L.yg_get_stream.argtypes = [P, ctypes.POINTER(P)]
+    L.yg_get_kernel_times.argtypes = [P, P]
+    L.yg_kernel_launch_count.restype = I64
+    L.yg_kernel_launch_count.argtypes = []
     _LIB = L
     return L
 
@@ -321,6 +325,12 @@ class IVisGridder:
     def synchronize(self):
         _check(self._lib.yg_synchronize(self.h))
 
+    def stream_handle(self) -> int:
+        """cudaStream_t (as an int) on which this gridder launches its kernels."""
+        sp = P()
+        _check(self._lib.yg_get_stream(self.h, ctypes.byref(sp)))
+        return sp.value or 0
+
     def set_tile(self, t: int):
         _check(self._lib.yg_set_tile(self.h, int(t)))
 
@@ -342,7 +352,7 @@ class IVisGridder:
         sizes = np.zeros(ncf, dtype=np.int32)
         offs = np.zeros(ncf, dtype=np.int64)
         _check(self._lib.yg_get_cf(self.h, sizes.ctypes.data, offs.ctypes.data, None, 0))
-        total = int(np.sum(sizes.astype(np.int64) ** 2))
+        total = int(np.max(offs + sizes.astype(np.int64) ** 2)) if ncf else 0
         data = np.zeros(total, dtype=np.complex64)
         _check(self._lib.yg_get_cf(self.h, sizes.ctypes.data, offs.ctypes.data, data.ctypes.data, total))
         out = []
@@ -380,12 +390,22 @@ class IVisGridder:
         per = nx * ny * npol * nchan
         return [buf[i * per:(i + 1) * per].reshape((nx, ny, npol, nchan), order="F") for i in range(n.value)]
 
+    def kernel_times(self):
+        out = np.zeros(4)
+        _check(self._lib.yg_get_kernel_times(self.h, out.ctypes.data))
+        return dict(kgrid_ms=out[0], kgrid_calls=out[1], kdegrid_ms=out[2], kdegrid_calls=out[3])
+
     def stats(self):
         out = np.zeros(8)
         _check(self._lib.yg_get_stats(self.h, out.ctypes.data))
         keys = ["samples_gridded", "taps_gridded", "samples_degridded", "taps_degridded", "ms_grid", "ms_degrid",
                 "ms_cf", "cf_planes"]
         return dict(zip(keys, out.tolist()))
+
+
+def kernel_launch_count() -> int:
+    """Process-wide number of the library's own kernel launches."""
+    return int(load().yg_kernel_launch_count())
 
 
 class VisGridderFactory:
