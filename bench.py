@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
+    ap.add_argument("--tile", type=int, default=0, help="uv tile side (0 = automatic)")
+    ap.add_argument("--variant", type=int, default=0, help="k_grid accumulation variant (0 = automatic)")
     return ap.parse_args()
 
 
@@ -314,6 +316,10 @@ def run_b200(args, w):
     model_buf = torch.zeros_like(d["vis"])
     acc_model = G.Accessor(d["uvw"], d["freq"], model_buf, shape=(d["nrow"], d["nchan"], npol))
     gg = G.VisGridderFactory.make(ps)
+    if args.tile:
+        gg.set_tile(args.tile)
+    if args.variant:
+        gg.set_grid_variant(args.variant)
     gg.initialiseGrid(axes, (nx, nx, npol, 1))
     gd = gg.clone()
     img = model_image(w, d["sky"], npol)

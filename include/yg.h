@@ -162,6 +162,8 @@ void yg_plan_destroy(yg_plan* plan);
 /* ---- tuning ---- */
 int yg_set_tile(yg_gridder* g, int32_t tile);      /* 0 = automatic */
 int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
+/* k_grid accumulation: 0 automatic, 1 in place in shared memory, 2 registers */
+int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */
 int yg_get_stream(yg_gridder* g, void** stream);

@@ -344,6 +344,13 @@ int yg_set_tile(yg_gridder* g, int32_t tile) {
   });
 }
 
+int yg_set_grid_variant(yg_gridder* g, int32_t variant) {
+  return guarded([&] {
+    if (variant < 0 || variant > 2) throw yg::YgError{YG_ERR_ARG, "variant must be 0, 1 or 2"};
+    G(g).set_grid_mode(variant);
+  });
+}
+
 int yg_set_item_size(yg_gridder* g, int32_t vmax) {
   return guarded([&] {
     if (vmax < 1) throw yg::YgError{YG_ERR_ARG, "item size must be positive"};

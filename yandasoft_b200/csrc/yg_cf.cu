@@ -63,7 +63,34 @@ CFView CFCacheDev::view() const {
   v.varsup = 0;
   for (int sz : h_size)
     if (sz != 0 && sz != maxsize) v.varsup = 1;
+  v.pad = pad.p ? pad.as<float2>() : nullptr;
+  v.wpad = wpad;
   return v;
+}
+
+// padded copy: plane c at c*wpad^2, taps beyond the plane's own size are 0
+__global__ void k_cf_pad(const float2* __restrict__ data, const long long* __restrict__ off,
+                         const int* __restrict__ size, int ncf, int wpad, float2* __restrict__ out) {
+  const long long per = (long long)wpad * wpad;
+  const long long total = per * ncf;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i / per);
+    const int t = (int)(i % per);
+    const int jx = t % wpad, jy = t / wpad;
+    const int w = size[c];
+    out[i] = (jx < w && jy < w) ? data[off[c] + jx + (long long)w * jy] : make_float2(0.f, 0.f);
+  }
+}
+
+int CFCacheDev::refresh_pad(cudaStream_t st) {
+  wpad = ((maxsize + 15) / 16) * 16;
+  if (ncf == 0 || wpad == 0) return YG_OK;
+  const long long total = (long long)wpad * wpad * ncf;
+  CF_TRY(pad.ensure(total * sizeof(float2)));
+  k_cf_pad<<<(int)std::min<long long>((total + 255) / 256, 148 * 64), 256, 0, st>>>(
+      data.as<float2>(), off.as<long long>(), size.as<int>(), ncf, wpad, pad.as<float2>());
+  CF_TRY(cudaGetLastError());
+  return YG_OK;
 }
 
 int CFCacheDev::layout(const std::vector<int>& sizes, const std::vector<int2>& offs) {
@@ -141,6 +168,9 @@ int cf_build_sphfunc(CFCacheDev& cache, int support, int os, double alpha) {
   }
   cache.support = support;
   CF_TRY(cudaMemcpy(cache.data.p, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  int rc = cache.refresh_pad(0);
+  if (rc) return rc;
+  CF_TRY(cudaDeviceSynchronize());
   return YG_OK;
 }
 
@@ -481,8 +511,10 @@ int cf_build_wproject(CFCacheDev& cache, const WProjCFParams& p, DevBuf& work, c
   k_normalise<<<(cache.ncf + 127) / 128, 128, 0, st>>>(cache.data.as<float2>(), cache.off.as<long long>(),
                                                       cache.size.as<int>(), cache.ncf);
   CF_TRY(cudaGetLastError());
-  CF_TRY(cudaStreamSynchronize(st));
   cache.support = its_support;
+  rc = cache.refresh_pad(st);
+  if (rc) return rc;
+  CF_TRY(cudaStreamSynchronize(st));
   return YG_OK;
 }
 
@@ -672,6 +704,10 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
   }
   cufftDestroy(plan1);
   cufftDestroy(planw);
+  if (rc == YG_OK) {
+    rc = cache.refresh_pad(st);
+    if (rc == YG_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = YG_ERR_CUDA;
+  }
   return rc;
 }
 

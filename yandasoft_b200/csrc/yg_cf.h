@@ -17,8 +17,12 @@ struct CFCacheDev {
   std::vector<int> h_size;
   std::vector<long long> h_off;
   std::vector<int2> h_offsets;
+  DevBuf pad;               // zero-padded wpad x wpad copy of every CF (gridding layout)
+  int wpad = 0;
   CFView view() const;
   int layout(const std::vector<int>& sizes, const std::vector<int2>& offs);
+  // rebuilds the padded copy from data; call after every change of the cache
+  int refresh_pad(cudaStream_t st);
   int download(std::vector<float2>& out) const;
 };
 
@@ -59,16 +63,18 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
 // gridding entry points (yg_gridding.cu)
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st);
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevError* err, cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
+              DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0 = nullptr,
+              cudaEvent_t ev1 = nullptr, int mode = 0);
 int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
               int nchan_img, double* sumw, DevError* err, cudaStream_t st);
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
                 cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
-size_t grid_smem_bytes(int npol, int P, int cfbuf);
-int grid_pols_per_pass(int npol, int P, int cfbuf);
-int grid_cf_buffer_bytes(int maxsize);
+size_t grid_smem_bytes(int npol, int Pg, int cfbuf);
+int grid_pols_per_pass(int npol, int Pg, int cfbuf);
+int grid_cf_buffer_bytes(int wpad);
+int grid_tile_stride(int tile, int wpad, int smax, bool varsup);
 extern std::atomic<long long> g_kernel_launches;
 
 }  // namespace yg

@@ -700,18 +700,22 @@ void Gridder::init_cf(const Chunk& dc) {
 // ---------------------------------------------------------------------------
 int Gridder::tile_for(int smax, int npol) const {
   if (tile_override_ > 0) return tile_override_;
-  // largest multiple of 8 whose padded tile, with the two CF buffers, fits
+  // largest multiple of 8 whose guttered tile and two padded CF buffers fit
   // ~110 KB of shared memory for the polarisations accumulated per pass (two
   // CTAs per SM), else 220 KB (one CTA per SM)
-  const int cfbuf = grid_cf_buffer_bytes(2 * smax + 1);
+  const int wpad = ((2 * smax + 1) + 15) / 16 * 16;
+  const bool varsup = cf_.view().varsup != 0;
+  const int cfbuf = grid_cf_buffer_bytes(wpad);
   const int budgets[2] = {110 * 1024, 220 * 1024};
   for (int b : budgets) {
     for (int npa : {npol, 2, 1}) {
       if (npa > npol || npol % npa) continue;
-      const double rest = (double)b - 2.0 * cfbuf - 4096.0;
+      const double rest = (double)b - 2.0 * cfbuf - 256.0;
       if (rest <= 0) continue;
-      const double pmax = std::sqrt(rest / (8.0 * npa));
-      const int t = ((int)pmax - 2 * smax) / 8 * 8;
+      const double pg2 = rest / (8.0 * npa) - 512.0;
+      if (pg2 <= 0) continue;
+      const int pgmax = (int)std::sqrt(pg2);
+      const int t = (pgmax - (wpad - 1) - (varsup ? smax : 0)) / 8 * 8;
       if (t >= 32) return std::min(t, 256);
     }
   }
@@ -880,8 +884,8 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
   rc_check(plan_sumw(pl, v, pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_, sumw_.as<double>(),
                      err_.as<DevError>(), stream_),
            "sum of weights");
-  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, scratch_, err_.as<DevError>(), stream_,
-                     k0, k1),
+  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, scratch_, svis_, err_.as<DevError>(),
+                     stream_, k0, k1, grid_mode_),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
   cudaEventRecord(e1, stream_);

@@ -110,6 +110,7 @@ class Gridder {
   void grid_plan(const Chunk& c, const Plan& pl);
   void degrid_plan(Chunk& c, Plan& pl);
   void set_tile(int t) { tile_override_ = t; }
+  void set_grid_mode(int m) { grid_mode_ = m; }
   int tile_for(int smax, int npol) const;
   int items_vmax() const { return vmax_; }
   void set_vmax(int v) { vmax_ = v; }
@@ -182,12 +183,13 @@ class Gridder {
   double rep_pointing_[2] = {0, 0};
   int tile_override_ = 0;
   int vmax_ = 0;   // samples per work item, 0 = automatic
+  int grid_mode_ = 0;  // k_grid accumulation variant, 0 = automatic
 
   CFCacheDev cf_;
   bool cf_built_ = false;
   DevBuf grids_, sumw_, carry_, err_, chanmap_d_, rowok_d_, corr_d_;
   DevBuf up_uvw_, up_delay_, up_freq_, up_vis_, up_noise_, up_flag_, up_feed_;
-  DevBuf scratch_, tmpvals_, cfwork_, img_tmp_, mfs_d_;
+  DevBuf scratch_, svis_, tmpvals_, cfwork_, img_tmp_, mfs_d_;
   int nsumw_rows_ = 1;
   Plan plan_;
   ImageFFT fft_;

@@ -241,6 +241,8 @@ __global__ void k_sumw(VisArgs v, const unsigned char* __restrict__ status, cons
 struct GridKArgs {
   const int4* items;
   const unsigned int* val;   // sample ids, sorted
+  const int4* rec;           // per sorted sample: cell, residues|w, cf index, sample id
+  const float2* svis;        // per sorted sample: npol weighted visibilities
   const int* runend;         // per sorted index at a run start: end of its run
   const unsigned int* pos;   // iu | iv << 16, unsorted (by sample id)
   const int* cfi;            // unsorted
@@ -249,7 +251,9 @@ struct GridKArgs {
   int tile, ntx;
   long long ntiles;
   int smax;                  // Smax of the plan
-  int P;                     // T + 2 Smax
+  int P;                     // T + 2 Smax: the padded tile written to scratch
+  int Pg;                    // row stride of the shared-memory tile, P plus a gutter
+  int Wp;                    // residue modulus: round_up(2 Smax + 1, 16)
   int cfbuf;                 // bytes of one shared-memory CF buffer
   float2* scratch;           // [item][npol][P][P]
   int pol0;                  // first polarisation of this pass
@@ -309,192 +313,212 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phas
 __host__ __device__ __forceinline__ unsigned cf_bytes(int w) { return (unsigned)(((w * w * 8) + 15) & ~15); }
 
 // Gridding of one work item.  CF planes are shared by runs of consecutive
-// samples (the sort key orders samples by CF inside a tile); each run's plane
-// is brought into shared memory by a TMA bulk copy one run ahead.
-template <int NPOL, int MAXSLOTS, bool VARSUP>
-__global__ void __launch_bounds__(kGridThreads) k_grid(GridKArgs a) {
+// samples (the sort key orders samples by CF inside a tile); each run's plane,
+// zero-padded to Wp x Wp with Wp = round_up(2 Smax + 1, 16), is brought into
+// shared memory by a TMA bulk copy two runs ahead, with full/empty mbarriers
+// between the copy (issued by thread 0) and the warps, so warps never meet at
+// a CTA-wide barrier inside the item.
+//
+// Thread/slot k owns the cells with (x mod Wp, y mod Wp) = (k mod Wp, k / Wp):
+// no two threads touch the same cell, so every tap is accumulated in place in
+// shared memory without atomics.  A half-warp holds 16 consecutive residues
+// of one row, so its CF taps and grid cells fall on 16 distinct banks (Wp and
+// the CF row stride are multiples of 16).  Taps of the padding are exact zeros
+// and land in the tile's gutter (columns/rows >= P), which is never read back.
+template <int NPOL, int MAXSLOTS>
+__global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int P = a.P;
-  const int P2 = P * P;
+  const int Pg = a.Pg;
+  const int PG2 = Pg * Pg + (int)blockDim.x;   // per polarisation: tile + one trash cell per thread
   float2* acc_s = reinterpret_cast<float2*>(smem_raw);
-  unsigned char* cfb = smem_raw + (size_t)NPOL * P2 * sizeof(float2);
+  unsigned char* cfb = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
   cfb = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(cfb) + 127) & ~(size_t)127);
   float2* cfs[2] = {reinterpret_cast<float2*>(cfb), reinterpret_cast<float2*>(cfb + a.cfbuf)};
-  VisRec* recs = reinterpret_cast<VisRec*>(cfb + 2 * (size_t)a.cfbuf);
-  float2* vals = reinterpret_cast<float2*>(recs + kBatch);
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(vals + kBatch * NPOL);
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(cfb + 2 * (size_t)a.cfbuf);
+  unsigned long long* empty = full + 2;
   __shared__ int s_abort;
+  const int nwarps = blockDim.x / 32;
+  const int lane = threadIdx.x & 31;
+  const int Wp = a.Wp;
+  const int Wp2 = Wp * Wp;
+  const int trash = Pg * Pg + threadIdx.x;      // target of slots beyond Wp^2
 
   const int4 it = a.items[blockIdx.x];
-  const long long t = (long long)it.x % a.ntiles;
-  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
-  const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
-  const int W = 2 * a.smax + 1;
-  const int W2 = W * W;
 
   if (threadIdx.x == 0) {
     s_abort = 0;
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], nwarps);
+    mbar_init(&empty[1], nwarps);
     mbar_fence_init();
   }
-  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
+  for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
   __syncthreads();
 
-  auto issue = [&](int start, int buf) {
-    const unsigned s = a.val[start];
-    const int c = a.cfi[s];
-    const unsigned bytes = cf_bytes(a.cf.size[c]);
-    mbar_expect_tx(&bars[buf], bytes);
-    bulk_g2s(cfs[buf], a.cf.data + a.cf.off[c], bytes, &bars[buf]);
-  };
-  // end of the run containing sorted index j, inside this item (always > j)
+  const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
   auto run_end = [&](int j) { return max(j + 1, min(a.runend[j], it.z)); };
+  auto issue = [&](int start, int buf) {
+    const int c = a.rec[start].z;
+    mbar_expect_tx(&full[buf], cfcopy);
+    bulk_g2s(cfs[buf], a.cf.pad + (size_t)c * Wp2, cfcopy, &full[buf]);
+  };
   if (threadIdx.x == 0) {
     issue(it.y, 0);
     const int e0 = run_end(it.y);
     if (e0 < it.z) issue(e0, 1);
   }
 
-  int rx[MAXSLOTS], ry[MAXSLOTS], cur[MAXSLOTS];
-  float2 acc[MAXSLOTS][NPOL];
+  int rx[MAXSLOTS], rowoff[MAXSLOTS];
+  bool live[MAXSLOTS];
 #pragma unroll
   for (int q = 0; q < MAXSLOTS; ++q) {
-    const int k = q * kGridThreads + threadIdx.x;
-    rx[q] = k < W2 ? k % W : -1;
-    ry[q] = k < W2 ? k / W : -1;
-    cur[q] = -1;
-#pragma unroll
-    for (int p = 0; p < NPOL; ++p) acc[q][p] = make_float2(0.f, 0.f);
+    const int k = q * blockDim.x + threadIdx.x;
+    live[q] = k < Wp2;
+    rx[q] = live[q] ? k % Wp : 0;
+    rowoff[q] = live[q] ? k / Wp : 0;   // ry
   }
 
-  const long long n = a.v.nrow * (long long)a.v.nchan;
-  unsigned phase[2] = {0u, 0u};
+  unsigned fphase[2] = {0u, 0u}, ephase[2] = {0u, 0u};
+  bool ok = true;
   int b = 0;
   for (int j = it.y; j < it.z;) {
     const int e = run_end(j);
-    if (!mbar_wait(&bars[b], phase[b])) {
-      if (threadIdx.x == 0) raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
-      s_abort = 1;
+    if (!mbar_wait(&full[b], fphase[b])) {
+      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+      ok = false;
+      break;
     }
-    phase[b] ^= 1u;
-    __syncthreads();
-    if (s_abort) break;
+    fphase[b] ^= 1u;
     const float2* __restrict__ cf_s = cfs[b];
-    for (int base = j; base < e; base += kBatch) {
-      const int nb = min(kBatch, e - base);
-      for (int jj = threadIdx.x; jj < nb; jj += blockDim.x) {
-        const unsigned int s = a.val[base + jj];
-        const unsigned int ps = a.pos[s];
-        const int c = a.cfi[s];
-        const int w = a.cf.size[c];
-        const int sup = (w - 1) / 2;
-        const int px0 = (int)(ps & 0xffffu) - sup - X0;
-        const int py0 = (int)(ps >> 16) - sup - Y0;
-        VisRec r;
-        r.cb = px0 + P * py0;
-        r.mx = px0 % W;
-        r.my = py0 % W;
-        r.w = w;
-        recs[jj] = r;
-        const long long row = s % a.v.nrow;
-        const int chan = (int)(s / a.v.nrow);
-        float pr, pi;
-        phasor_of(a.v, row, chan, &pr, &pi);
-        const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+    int4 r = a.rec[j];
+    float2 vv[NPOL];
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) vv[p] = a.svis[(size_t)j * a.npol_total + a.pol0 + p];
+    for (int i = j; i < e; ++i) {
+      // prefetch the next sample's record while this one is gridded
+      int4 rn = r;
+      float2 vn[NPOL];
+      if (i + 1 < e) {
+        rn = a.rec[i + 1];
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) vn[p] = a.svis[(size_t)(i + 1) * a.npol_total + a.pol0 + p];
+      }
+      const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
+      const int cb = px0 + Pg * py0;
+      const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
+#pragma unroll
+      for (int q = 0; q < MAXSLOTS; ++q) {
+        int jx = rx[q] - mx;
+        jx += (jx < 0) ? Wp : 0;
+        int jy = rowoff[q] - my;
+        jy += (jy < 0) ? Wp : 0;
+        const int cell = live[q] ? cb + jx + Pg * jy : trash;
+        const float2 c = cf_s[live[q] ? jx + Wp * jy : 0];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) {
-          const int pp = a.pol0 + p;
-          const float nre = a.v.noise ? a.v.noise[s + n * pp].x : 1.f;
-          const float wt = noise_weight(nre);
-          float2 o;
-          if (a.v.psf) {
-            o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
-            o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
-          } else {
-            const float2 vv = a.v.vis[s + n * pp];
-            const float vr = vv.x, vi = -vv.y;
-            float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
-            float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
-            rr = __fmul_rn(__fmul_rn(rr, wt), m);
-            ri = __fmul_rn(__fmul_rn(ri, wt), m);
-            o = make_float2(rr, ri);
-          }
-          vals[jj * NPOL + p] = o;
+          float2 g = acc_s[p * PG2 + cell];
+          g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
+          g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
+          acc_s[p * PG2 + cell] = g;
         }
       }
-      __syncthreads();
-      for (int jj = 0; jj < nb; ++jj) {
-        const VisRec r = recs[jj];
-        float2 vv[NPOL];
+      r = rn;
 #pragma unroll
-        for (int p = 0; p < NPOL; ++p) vv[p] = vals[jj * NPOL + p];
-#pragma unroll
-        for (int q = 0; q < MAXSLOTS; ++q) {
-          if (rx[q] < 0) continue;
-          int jx = rx[q] - r.mx;
-          jx += (jx < 0) ? W : 0;
-          int jy = ry[q] - r.my;
-          jy += (jy < 0) ? W : 0;
-          if (VARSUP && (jx >= r.w || jy >= r.w)) continue;
-          const int cell = r.cb + jx + P * jy;
-          const float2 c = cf_s[jx + r.w * jy];
-          if (cell != cur[q]) {
-            if (cur[q] >= 0) {
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p) {
-                float2 g = acc_s[p * P2 + cur[q]];
-                g.x += acc[q][p].x;
-                g.y += acc[q][p].y;
-                acc_s[p * P2 + cur[q]] = g;
-                acc[q][p] = make_float2(0.f, 0.f);
-              }
-            }
-            cur[q] = cell;
-          }
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            acc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, acc[q][p].x));
-            acc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, acc[q][p].y));
-          }
-        }
-      }
-      __syncthreads();
+      for (int p = 0; p < NPOL; ++p) vv[p] = vn[p];
     }
-    // buffer b is free: bring the run after the next one into it
+    // this warp is done with buffer b
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
+    // producer: refill buffer b with the run after the next one
     if (threadIdx.x == 0 && e < it.z) {
       const int e2 = run_end(e);
       if (e2 < it.z) {
-        fence_proxy_async_smem();
-        issue(e2, b);
+        if (!mbar_wait(&empty[b], ephase[b])) {
+          raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+          s_abort = 1;
+        } else {
+          fence_proxy_async_smem();
+          issue(e2, b);
+        }
       }
     }
+    ephase[b] ^= 1u;
     j = e;
     b ^= 1;
+    if (s_abort) {
+      ok = false;
+      break;
+    }
   }
-  if (s_abort) {
+  if (!ok) {
     // let any copy still in flight land before the CTA's shared memory goes away
     if (threadIdx.x == 0) {
-      mbar_wait(&bars[0], phase[0]);
-      mbar_wait(&bars[1], phase[1]);
+      mbar_wait(&full[0], fphase[0]);
+      mbar_wait(&full[1], fphase[1]);
     }
-    return;
-  }
-#pragma unroll
-  for (int q = 0; q < MAXSLOTS; ++q) {
-    if (cur[q] >= 0) {
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        float2 g = acc_s[p * P2 + cur[q]];
-        g.x += acc[q][p].x;
-        g.y += acc[q][p].y;
-        acc_s[p * P2 + cur[q]] = g;
-      }
-    }
+    s_abort = 1;
   }
   __syncthreads();
+  if (s_abort) return;
+  const int P = a.P, P2 = P * P;
   float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
-  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) out[i] = acc_s[i];
+  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
+    const int p = i / P2, c = i % P2;
+    out[i] = acc_s[p * PG2 + (c % P) + Pg * (c / P)];
+  }
+}
+
+// Per sorted sample, once per plan: the footprint origin cell inside the
+// padded tile, its residues mod W and the CF width, the CF index, the sample id.
+__global__ void k_records(const unsigned int* __restrict__ val, const unsigned int* __restrict__ pos,
+                          const int* __restrict__ cfi, const unsigned long long* __restrict__ key, long long nvalid,
+                          int mbits, int ncf, long long ntiles, int ntx, int tile, int smax, int Wp,
+                          const int* __restrict__ cfsize, int4* __restrict__ rec) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned int s = val[i];
+    const unsigned int ps = pos[s];
+    const int c = cfi[s];
+    const int w = cfsize[c];
+    const int sup = (w - 1) / 2;
+    const long long t = key_tile(key[i], mbits, ncf) % ntiles;
+    const int tx = (int)(t % ntx), ty = (int)(t / ntx);
+    const int px0 = (int)(ps & 0xffffu) - sup - (tx * tile - smax);
+    const int py0 = (int)(ps >> 16) - sup - (ty * tile - smax);
+    rec[i] = make_int4(px0 | (py0 << 16), (px0 % Wp) | ((py0 % Wp) << 10) | (w << 20), c, (int)s);
+  }
+}
+
+// Per sorted sample, once per grid pass: rVis = phasor * conj(vis) * wt (* mfs)
+// (TableVisGridder.cc:775-806), or wt (* mfs) for the PSF.
+__global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long nvalid, float2* __restrict__ out) {
+  const long long n = v.nrow * (long long)v.nchan;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
+    const long long s = rec[i].w;
+    const long long row = s % v.nrow;
+    const int chan = (int)(s / v.nrow);
+    float pr, pi;
+    phasor_of(v, row, chan, &pr, &pi);
+    const float m = v.mfs ? v.mfs[chan] : 1.f;
+    for (int p = 0; p < v.npol; ++p) {
+      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
+      const float wt = noise_weight(nre);
+      float2 o;
+      if (v.psf) {
+        o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
+        o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
+      } else {
+        const float2 vv = v.vis[s + n * p];
+        const float vr = vv.x, vi = -vv.y;
+        float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+        float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+        rr = __fmul_rn(__fmul_rn(rr, wt), m);
+        ri = __fmul_rn(__fmul_rn(ri, wt), m);
+        o = make_float2(rr, ri);
+      }
+      out[(size_t)i * v.npol + p] = o;
+    }
+  }
 }
 
 // Run ends of the sorted list (a run = consecutive samples of one tile with
@@ -594,6 +618,7 @@ __global__ void k_halo_sum(HaloArgs a) {
 // ---------------------------------------------------------------------------
 struct DegridKArgs {
   const int4* items;
+  const int4* rec;
   const unsigned int* val;
   const unsigned int* pos;
   const int* cfi;
@@ -649,15 +674,13 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
   const float2* src = a.smem_grid ? g_s : gbase;
   const long long pstride = a.smem_grid ? P2 : plane_cells;
   for (int i = it.y + warp; i < it.z; i += nwarps) {
-    const unsigned int s = a.val[i];
-    const unsigned int ps = a.pos[s];
-    const int c = a.cfi[s];
-    const int w = a.cf.size[c];
-    const int sup = (w - 1) / 2;
-    const int px0 = (int)(ps & 0xffffu) - sup;
-    const int py0 = (int)(ps >> 16) - sup;
-    const long long origin = a.smem_grid ? (long long)(px0 - X0) + (long long)P * (py0 - Y0)
-                                         : (long long)px0 + (long long)a.nx * py0;
+    const int4 r = a.rec[i];
+    const unsigned int s = (unsigned int)r.w;
+    const int c = r.z;
+    const int w = (r.y >> 20) & 1023;
+    const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
+    const long long origin = a.smem_grid ? (long long)px0 + (long long)P * py0
+                                         : (long long)(X0 + px0) + (long long)a.nx * (Y0 + py0);
     const float2* __restrict__ cfp = a.cf.data + a.cf.off[c];
     float re[4][NPOL], im[4][NPOL];
 #pragma unroll
@@ -905,67 +928,115 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     k_run_unreverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(revmin, pl.nvalid, pl.runend.as<int>());
     YG_COUNT_LAUNCH();
   }
+  YG_CUDA_TRY(pl.rec.ensure((size_t)std::max(1ll, pl.nvalid) * sizeof(int4)));
+  if (pl.nvalid > 0) {
+    if (a.cf.wpad > 1023 || !a.cf.pad) return YG_ERR_UNSUPPORTED;  // residues are packed in 10 bits
+    k_records<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.val.as<unsigned int>(), pl.pos.as<unsigned int>(),
+                                                        pl.cfi.as<int>(), pl.key.as<unsigned long long>(), pl.nvalid,
+                                                        a.mbits, a.cf.ncf, (long long)a.ntx * a.nty, a.ntx, a.tile,
+                                                        pl.smax, a.cf.wpad, a.cf.size, pl.rec.as<int4>());
+    YG_COUNT_LAUNCH();
+  }
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
 
-static int max_slots_for(int W, int threads) { return (W * W + threads - 1) / threads; }
 
 template <int NPOL, int MAXSLOTS>
-static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, size_t smem, bool varsup, cudaStream_t st) {
-  if (varsup) {
-    auto k = k_grid<NPOL, MAXSLOTS, true>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<nitems, kGridThreads, smem, st>>>(g);
-  } else {
-    auto k = k_grid<NPOL, MAXSLOTS, false>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<nitems, kGridThreads, smem, st>>>(g);
-  }
+static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
+  auto k = k_grid<NPOL, MAXSLOTS>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<nitems, threads, smem, st>>>(g);
   YG_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
+// threads x slots covering Wp^2 residue classes with the least waste
+// (threads a multiple of 32, at most 512)
+struct GridShape {
+  int threads, slots;
+};
+
+GridShape grid_shape(int Wp) {
+  const int W2 = Wp * Wp;
+  const int cand[10] = {1, 2, 3, 4, 6, 8, 9, 12, 16, 25};
+  GridShape best{0, 0};
+  long long best_waste = -1;
+  for (int sl : cand) {
+    int th = ((W2 + sl - 1) / sl + 31) / 32 * 32;
+    if (th < 64) th = 64;
+    if (th > 512) continue;
+    const long long waste = (long long)th * sl - W2;
+    if (best_waste < 0 || waste < best_waste || (waste == best_waste && th > best.threads)) {
+      best = GridShape{th, sl};
+      best_waste = waste;
+    }
+  }
+  return best;
+}
+
 template <int NPOL>
-static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, int slots, bool varsup,
-                                  cudaStream_t st) {
-  if (slots <= 4) return launch_grid_ms<NPOL, 4>(g, nitems, smem, varsup, st);
-  if (slots <= 8) return launch_grid_ms<NPOL, 8>(g, nitems, smem, varsup, st);
-  if (slots <= 16) return launch_grid_ms<NPOL, 16>(g, nitems, smem, varsup, st);
+static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, GridShape sh, cudaStream_t st) {
+  const int t = sh.threads;
+  switch (sh.slots) {
+    case 1: return launch_grid_ms<NPOL, 1>(g, nitems, t, smem, st);
+    case 2: return launch_grid_ms<NPOL, 2>(g, nitems, t, smem, st);
+    case 3: return launch_grid_ms<NPOL, 3>(g, nitems, t, smem, st);
+    case 4: return launch_grid_ms<NPOL, 4>(g, nitems, t, smem, st);
+    case 6: return launch_grid_ms<NPOL, 6>(g, nitems, t, smem, st);
+    case 8: return launch_grid_ms<NPOL, 8>(g, nitems, t, smem, st);
+    case 9: return launch_grid_ms<NPOL, 9>(g, nitems, t, smem, st);
+    case 12: return launch_grid_ms<NPOL, 12>(g, nitems, t, smem, st);
+    case 16: return launch_grid_ms<NPOL, 16>(g, nitems, t, smem, st);
+    case 25: return launch_grid_ms<NPOL, 25>(g, nitems, t, smem, st);
+    default: break;
+  }
   return cudaErrorInvalidConfiguration;
 }
 
-// bytes of one shared-memory CF buffer for CFs of at most maxsize^2 taps
-int grid_cf_buffer_bytes(int maxsize) { return (int)((cf_bytes(maxsize) + 127u) & ~127u); }
+// shared memory of k_grid: the guttered tile (Pg^2 + one trash cell per
+// thread) per polarisation, two padded CF buffers (Wp^2 taps) and 4 mbarriers
+int grid_cf_buffer_bytes(int wpad) { return ((wpad * wpad * 8) + 127) / 128 * 128; }
 
-size_t grid_smem_bytes(int npol, int P, int cfbuf) {
-  return (size_t)npol * P * P * sizeof(float2) + 128 + 2 * (size_t)cfbuf + kBatch * sizeof(VisRec) +
-         (size_t)kBatch * npol * sizeof(float2) + 2 * sizeof(unsigned long long);
+int grid_tile_stride(int tile, int wpad, int smax, bool varsup) { return tile + wpad - 1 + (varsup ? smax : 0); }
+
+size_t grid_smem_bytes(int npol, int Pg, int cfbuf) {
+  return (size_t)npol * ((size_t)Pg * Pg + 512) * sizeof(float2) + 128 + 2 * (size_t)cfbuf +
+         4 * sizeof(unsigned long long);
 }
 
 // Polarisations accumulated together in one k_grid pass: the most that fit
 // the shared-memory budget.
-int grid_pols_per_pass(int npol, int P, int cfbuf) {
+int grid_pols_per_pass(int npol, int Pg, int cfbuf) {
   const int cands[3] = {4, 2, 1};
   for (int c : cands) {
     if (c > npol || npol % c) continue;
-    if (grid_smem_bytes(c, P, cfbuf) <= 227 * 1024) return c;
+    if (grid_smem_bytes(c, Pg, cfbuf) <= 227 * 1024) return c;
   }
   return 0;
 }
 
 // Grids the samples of a plan onto `grid` (ngrid planes of (nx, ny, npol, nchan_img)).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevError* err, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
+              DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+              int mode) {
+  (void)mode;
   if (pl.nitems == 0) return YG_OK;
+  if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
   const int P = pl.pad;
-  const int W = 2 * pl.smax + 1;
-  const int slots = max_slots_for(W, kGridThreads);
+  const int Pg = grid_tile_stride(pl.tile, cf.wpad, pl.smax, cf.varsup != 0);
+  const GridShape shape = grid_shape(cf.wpad);
+  if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
   const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
+  YG_CUDA_TRY(svis.ensure((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
+  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>());
+  YG_COUNT_LAUNCH();
   GridKArgs g;
   g.items = pl.items.as<int4>();
   g.val = pl.val.as<unsigned int>();
+  g.rec = pl.rec.as<int4>();
+  g.svis = svis.as<float2>();
   g.runend = pl.runend.as<int>();
   g.pos = pl.pos.as<unsigned int>();
   g.cfi = pl.cfi.as<int>();
@@ -976,21 +1047,23 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.ntiles = (long long)pl.ntx * pl.nty;
   g.smax = pl.smax;
   g.P = P;
-  g.cfbuf = grid_cf_buffer_bytes(cf.maxsize);
+  g.Pg = Pg;
+  g.Wp = cf.wpad;
+  g.cfbuf = grid_cf_buffer_bytes(cf.wpad);
   g.scratch = scratch.as<float2>();
   g.npol_total = v.npol;
   g.err = err;
-  const int npa = grid_pols_per_pass(v.npol, P, g.cfbuf);
+  const int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf);
   if (npa == 0) return YG_ERR_UNSUPPORTED;
-  const size_t smem = grid_smem_bytes(npa, P, g.cfbuf);
+  const size_t smem = grid_smem_bytes(npa, Pg, g.cfbuf);
   if (ev0) cudaEventRecord(ev0, st);
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
     cudaError_t e;
     switch (npa) {
-      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
-      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
-      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, slots, cf.varsup != 0, st); break;
+      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st); break;
+      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st); break;
+      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, shape, st); break;
       default: return YG_ERR_UNSUPPORTED;
     }
     if (e != cudaSuccess) return YG_ERR_CUDA;
@@ -1039,6 +1112,7 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
   if (pl.nitems > 0) {
     DegridKArgs d;
     d.items = pl.items.as<int4>();
+    d.rec = pl.rec.as<int4>();
     d.val = pl.val.as<unsigned int>();
     d.pos = pl.pos.as<unsigned int>();
     d.cfi = pl.cfi.as<int>();

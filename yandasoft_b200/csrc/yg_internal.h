@@ -51,6 +51,8 @@ struct CFView {
   int noffsets = 0;
   int maxsize = 0;                 // max 2S+1 over the cache
   int varsup = 0;                  // 1 when CF sizes differ (variable support)
+  const float2* pad = nullptr;      // every CF zero-padded to wpad x wpad (row stride wpad)
+  int wpad = 0;                    // round_up(maxsize, 16)
 };
 
 // How a (row, chan, feed) sample maps to a CF plane and a grid.
@@ -102,7 +104,8 @@ struct Plan {
   DevBuf tstart, tend, nit, itembase, items, nvalid_d, sort_tmp;
   DevBuf order_prev;            // degrid stale-value scan
   DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
-  DevBuf runend;                // end of each run of equal (tile, CF) samples, at its start
+  DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
+  DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
   double taps = 0;              // sum of (2S+1)^2 over valid samples (per pol)
 };
 

@@ -36,6 +36,7 @@ EXPORTS = [
     "yg_get_sum_weights", "yg_get_grid", "yg_get_shape", "yg_get_stats", "yg_build_cf", "yg_plan_create",
     "yg_plan_grid", "yg_plan_degrid", "yg_plan_info", "yg_plan_samples", "yg_plan_destroy", "yg_set_tile", "yg_set_item_size",
     "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
+    "yg_set_grid_variant",
 ]
 
 
@@ -98,6 +99,7 @@ def load(path: str | None = None):
     L.yg_plan_destroy.restype = None
     L.yg_set_tile.argtypes = [P, I32]
     L.yg_set_item_size.argtypes = [P, I32]
+    L.yg_set_grid_variant.argtypes = [P, I32]
     L.yg_synchronize.argtypes = [P]
     L.yg_get_stream.argtypes = [P, ctypes.POINTER(P)]
     L.yg_get_kernel_times.argtypes = [P, P]
@@ -333,6 +335,9 @@ class IVisGridder:
 
     def set_tile(self, t: int):
         _check(self._lib.yg_set_tile(self.h, int(t)))
+
+    def set_grid_variant(self, v: int):
+        _check(self._lib.yg_set_grid_variant(self.h, int(v)))
 
     def set_item_size(self, v: int):
         _check(self._lib.yg_set_item_size(self.h, int(v)))
