@@ -168,6 +168,25 @@ int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */
 int yg_get_stream(yg_gridder* g, void** stream);
 
+/* ---- degridding without device allocation ----
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code that records its major cycle into a CUDA graph while a stream is being
+ * captured (device allocation cannot be captured), or an application that
+ * fixes the GPU's memory budget at start-up and forbids later allocations.
+ * Same semantics as yg_degrid for a device-resident chunk (on_device = 1):
+ * the model visibilities are added into chunk->vis.  The gridder must have
+ * its convolution functions built (yg_build_cf, or one earlier yg_degrid) and
+ * its model grid initialised (yg_initialise_degrid); both stay owned by the
+ * handle.  Every temporary of the call lives in one static device array of
+ * about 60 MB that each GPU loading the library holds until exit; the call
+ * takes at most 2^20 rows x channels (YG_ERR_ARG beyond that), 1, 2 or 4
+ * polarisations and 65536 channels, and allocates nothing.  The array's
+ * device address is looked up the first time the call runs on a device, so
+ * make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race on it and must be serialised by the caller. */
+int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk);
+
 #ifdef __cplusplus
 }
 #endif

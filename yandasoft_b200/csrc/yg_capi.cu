@@ -371,4 +371,11 @@ int yg_synchronize(yg_gridder* g) {
   return guarded([&] { G(g).sync(); });
 }
 
+int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk) {
+  return guarded([&] {
+    yg::Chunk c = to_chunk(chunk);
+    G(g).degrid_noalloc(c);
+  });
+}
+
 }  // extern "C"

@@ -121,6 +121,8 @@ class Gridder {
     ensure_device();
     init_cf(c);
   }
+  // degrid of a device-resident chunk with no device allocation (yg_noalloc.cu)
+  void degrid_noalloc(Chunk& c);
   // per-sample on-grid position (with CF offset), CF index and status of a plan
   void plan_samples(const Plan& pl, int* iu, int* iv, int* cfi, unsigned char* status) const;
 
@@ -198,5 +200,10 @@ class Gridder {
   int device_ = 0;
   bool device_ready_ = false;
 };
+
+// size of the static device array used by Gridder::degrid_noalloc and the
+// largest rows x channels it accepts per call
+size_t noalloc_scratch_bytes();
+long long noalloc_max_samples();
 
 }  // namespace yg

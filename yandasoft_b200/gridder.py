@@ -36,7 +36,7 @@ EXPORTS = [
     "yg_get_sum_weights", "yg_get_grid", "yg_get_shape", "yg_get_stats", "yg_build_cf", "yg_plan_create",
     "yg_plan_grid", "yg_plan_degrid", "yg_plan_info", "yg_plan_samples", "yg_plan_destroy", "yg_set_tile", "yg_set_item_size",
     "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
-    "yg_set_grid_variant",
+    "yg_set_grid_variant", "yg_degrid_noalloc",
 ]
 
 
@@ -100,6 +100,7 @@ def load(path: str | None = None):
     L.yg_set_tile.argtypes = [P, I32]
     L.yg_set_item_size.argtypes = [P, I32]
     L.yg_set_grid_variant.argtypes = [P, I32]
+    L.yg_degrid_noalloc.argtypes = [P, ctypes.POINTER(yg_chunk)]
     L.yg_synchronize.argtypes = [P]
     L.yg_get_stream.argtypes = [P, ctypes.POINTER(P)]
     L.yg_get_kernel_times.argtypes = [P, P]
@@ -296,6 +297,12 @@ class IVisGridder:
     def degrid(self, acc: Accessor):
         c = acc.c()
         _check(self._lib.yg_degrid(self.h, ctypes.byref(c)))
+
+    def degrid_noalloc(self, acc: Accessor):
+        """degrid() for a device-resident chunk that allocates no device memory
+        (scratch in a static device array; see include/yg.h)."""
+        c = acc.c()
+        _check(self._lib.yg_degrid_noalloc(self.h, ctypes.byref(c)))
 
     def finaliseDegrid(self):
         _check(self._lib.yg_finalise_degrid(self.h))
