@@ -82,6 +82,8 @@ def _setup(L):
     L.orc_generic.argtypes = [ctypes.POINTER(_Cfg), I64, I32, I32, P, P, P, P, P, P, P, P, P, P, P, P,
                               P, P, P, ctypes.POINTER(_Stats), I64]
     L.orc_last_error.restype = ctypes.c_char_p
+    L.orc_wstack_wproj_map.restype = I32
+    L.orc_wstack_wproj_map.argtypes = [I64, I32, P, P, I32, D, I32, I32, D, P, P]
     L.orc_dft.restype = I32
     L.orc_dft.argtypes = [I64, I32, P, P, I32, P, P, P, I32]
 
@@ -230,6 +232,11 @@ class OracleGridder:
             self.ws = WSampling(int(kw.get("nwplanes", 65)), float(kw.get("wmax", default_wmax)),
                                 kw.get("wsampling", "linear"), float(kw.get("exponent", 1.0)),
                                 float(kw.get("nwplanes50", 0.0)), bool(kw.get("wmaxclip", False)))
+        elif kind == "WStackWProject":
+            # w-stacks over (-wmax, wmax); w-projection of the residual over half a stack spacing
+            self.stacks = WSampling(int(kw.get("nwstacks", 17)), float(kw.get("wmax", 35000.0)),
+                                    wmaxclip=bool(kw.get("wmaxclip", False)))
+            self.ws = WSampling(int(kw.get("nwplanes", 33)), 0.5 * self.stacks.wscale)
         else:
             self.ws = None
 
@@ -245,7 +252,11 @@ class OracleGridder:
         return frequency_map(freq, self.nchan_img, self.freq_axis[0], self.freq_axis[1])
 
     def _ngrids(self):
-        return self.ws.nwplanes if self.kind == "WStack" else 1
+        if self.kind == "WStack":
+            return self.ws.nwplanes
+        if self.kind == "WStackWProject":
+            return self.stacks.nwplanes
+        return 1
 
     def initialise_grid(self, nx, ny, npol, nchan, cell_x, cell_y, freq_axis=None, dopsf=False):
         self._init_axes(nx, ny, npol, nchan, cell_x, cell_y, freq_axis)
@@ -258,8 +269,10 @@ class OracleGridder:
         self.rep_pointing = None
 
     def _nsumw_cf(self):
-        if self.kind in ("WProject", "WStack"):
+        if self.kind in ("WProject", "WStackWProject"):
             return self.ws.nwplanes
+        if self.kind == "WStack":
+            return 1
         if self.kind == "AWProject":
             return None  # set when the CF cache is built
         return 1
@@ -280,7 +293,7 @@ class OracleGridder:
                       variablesupport=bool(kw.get("variablesupport", False)),
                       offsetsupport=bool(kw.get("offsetsupport", False)),
                       cutoff_absolute=bool(kw.get("cutoff_absolute", False)), wterms=self.ws.wterms())
-        if self.kind == "WProject":
+        if self.kind in ("WProject", "WStackWProject"):
             return cfmod.WProjectParams(maxsupport=int(kw.get("maxsupport", 256)), **common)
         return cfmod.AWProjectParams(maxsupport=int(kw.get("maxsupport", 128)),
                                      diameter=float(kw.get("diameter", 12.0)), blockage=float(kw.get("blockage", 2.0)),
@@ -297,7 +310,7 @@ class OracleGridder:
             if self.kind == "WStack":
                 self.os = os_
             self.cache = cfmod.sphfunc_cf(sup, os_, self.alpha)
-        elif self.kind == "WProject":
+        elif self.kind in ("WProject", "WStackWProject"):
             self.cache = cfmod.wproject_cf(self.nx, self.ny, self.uvcell[0], self.uvcell[1], self._cf_params())
         else:
             if self.cache is None:
@@ -323,6 +336,15 @@ class OracleGridder:
         nrow, nchan = chunk.nrow, len(chunk.freq)
         if self.kind == "SphFunc":
             return None, None
+        if self.kind == "WStackWProject":
+            uvw = np.ascontiguousarray(chunk.uvw, dtype=np.float64)
+            freq = np.ascontiguousarray(chunk.freq, dtype=np.float64)
+            gmap = np.zeros((nrow, nchan), dtype=np.int32, order="F")
+            cmap = np.zeros((nrow, nchan), dtype=np.int32, order="F")
+            _check(lib().orc_wstack_wproj_map(nrow, nchan, _p(uvw), _p(freq), self.stacks.nwplanes,
+                                              self.stacks.wscale, int(self.stacks.wmaxclip), self.ws.nwplanes,
+                                              self.ws.wscale, _p(gmap), _p(cmap)))
+            return cmap, gmap
         planes = self.ws.plane_map(chunk.uvw, chunk.freq)
         if self.kind == "WStack":
             return np.zeros((nrow, nchan), dtype=np.int32, order="F"), planes
@@ -401,10 +423,14 @@ class OracleGridder:
         self.init_cf(chunk)
         return self._run(chunk, forward=False)
 
+    def _stack_sampling(self):
+        return self.ws if self.kind == "WStack" else self.stacks
+
     def finalise_grid(self):
-        if self.kind == "WStack":
-            screens = [cfmod.wstack_screen(self.nx, self.ny, self.uvcell[0], self.uvcell[1], self.ws.wterm(i))
-                       for i in range(self.ws.nwplanes)]
+        if self.kind in ("WStack", "WStackWProject"):
+            st = self._stack_sampling()
+            screens = [cfmod.wstack_screen(self.nx, self.ny, self.uvcell[0], self.uvcell[1], st.wterm(i))
+                       for i in range(st.nwplanes)]
             return cfmod.finalise_grid(self.grids, self.grdsf, screens=screens)
         if self.kind == "AWProject" and not self.aw_params.spheroidaltaper:
             s = None
@@ -423,9 +449,10 @@ class OracleGridder:
         self._init_axes(nx, ny, npol, nchan, cell_x, cell_y, freq_axis)
         self.psf = False
         self.model_empty = not np.max(np.abs(image)) > 0
-        if self.kind == "WStack":
-            screens = [cfmod.wstack_screen(nx, ny, self.uvcell[0], self.uvcell[1], self.ws.wterm(i))
-                       for i in range(self.ws.nwplanes)]
+        if self.kind in ("WStack", "WStackWProject"):
+            st = self._stack_sampling()
+            screens = [cfmod.wstack_screen(nx, ny, self.uvcell[0], self.uvcell[1], st.wterm(i))
+                       for i in range(st.nwplanes)]
             self.grids = cfmod.wstack_initialise_degrid(image, self.grdsf, screens)
         elif self.kind == "AWProject" and not self.kw.get("spheroidaltaper", False):
             self.grids = [cfmod.fft2d(image.astype(np.complex64), True)]

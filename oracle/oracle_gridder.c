@@ -196,6 +196,41 @@ int orc_wplane_map(int64_t nrow, int nchan, const double *uvw, const double *fre
     return ORC_OK;
 }
 
+/* W-stacking + W-projection composition: the grid plane is the w-stack of
+ * w (WDependentGridderBase::getWPlane over the stack sampling), the CF plane
+ * is getWPlane of the residual w - wterm(stack) over the projection sampling
+ * (half a stack spacing).  gmap/cmap are (row, chan), row fastest. */
+int orc_wstack_wproj_map(int64_t nrow, int nchan, const double *uvw, const double *freq,
+                         int nstacks, double sscale, int swmaxclip,
+                         int nwplanes, double wscale, int32_t *gmap, int32_t *cmap)
+{
+    orc_wcfg cs, cp;
+    int64_t i;
+    int ch, err = 0;
+    memset(&cs, 0, sizeof cs);
+    memset(&cp, 0, sizeof cp);
+    cs.nwplanes = nstacks; cs.wscale = sscale; cs.sampling = ORC_WS_LINEAR; cs.wmaxclip = swmaxclip;
+    cp.nwplanes = nwplanes; cp.wscale = wscale; cp.sampling = ORC_WS_LINEAR; cp.wmaxclip = 0;
+    for (i = 0; i < nrow; ++i) {
+        const double w = uvw[3 * i + 2] / ORC_C;
+        for (ch = 0; ch < nchan; ++ch) {
+            const double wf = w * freq[ch];
+            const int g = orc_get_wplane(&cs, wf, &err);
+            int c = -1;
+            if (err) return err;
+            if (g >= 0) {
+                const int half = (nstacks - 1) / 2;
+                const double wst = (double)(g - half) * sscale;
+                c = orc_get_wplane(&cp, wf - wst, &err);
+                if (err) return err;
+            }
+            gmap[i + nrow * ch] = g;
+            cmap[i + nrow * ch] = c;
+        }
+    }
+    return ORC_OK;
+}
+
 /* ---------------------------------------------------------------------- */
 /* index block of TableVisGridder::generic                                */
 /* ---------------------------------------------------------------------- */

@@ -677,9 +677,11 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
               if (rc) break;
             }
           }
-          sup[iw] = p.variablesupport ? s : cache.support;
+          if (p.variablesupport) sup[iw] = s;
           if (p.offsetsupport) offs[iw] = make_int2(ou, ov);
         }
+        // fixed support: every plane takes the support found on the first one
+        if (!p.variablesupport) sup[iw] = cache.support;
         rc = check_overflow(sup[iw], offs[iw].x, offs[iw].y, os, nx, ny);
         if (rc) break;
       }

@@ -62,11 +62,11 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
 
 // gridding entry points (yg_gridding.cu)
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st);
+// Grids the samples of a plan and, when sw.sumw is set, adds their weights into
+// the sums of weights (one fused pass over the sorted samples).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0 = nullptr,
-              cudaEvent_t ev1 = nullptr, int mode = 0);
-int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
-              int nchan_img, double* sumw, DevError* err, cudaStream_t st);
+              const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st,
+              cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, int mode = 0);
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
                 cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);

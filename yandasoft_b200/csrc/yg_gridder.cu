@@ -881,11 +881,9 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
   cudaEventCreate(&k0);
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  rc_check(plan_sumw(pl, v, pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_, sumw_.as<double>(),
-                     err_.as<DevError>(), stream_),
-           "sum of weights");
-  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, scratch_, svis_, err_.as<DevError>(),
-                     stream_, k0, k1, grid_mode_),
+  const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
+  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
+                     err_.as<DevError>(), stream_, k0, k1, grid_mode_),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
   cudaEventRecord(e1, stream_);

@@ -212,29 +212,6 @@ __device__ __forceinline__ void phasor_of(const VisArgs& v, long long row, int c
   *pi = (float)sin(ph);
 }
 
-// sum of weights per (row, pol, image channel), double (TableVisGridder.cc:783-823)
-__global__ void k_sumw(VisArgs v, const unsigned char* __restrict__ status, const int* __restrict__ cfi,
-                       const int* __restrict__ chan_map, int os, int track_per_os, int nrows_sumw, int nchan_img,
-                       double* __restrict__ sumw, DevError* err) {
-  const long long n = v.nrow * (long long)v.nchan;
-  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-    if (status[s] != 3) continue;
-    const long long row = s % v.nrow;
-    if (v.psf && v.psf_ok && !v.psf_ok[row]) continue;
-    const int chan = (int)(s / v.nrow);
-    const int c = cfi[s];
-    const int r = track_per_os ? c : c / (os * os);
-    const int ic = chan_map[chan];
-    if (r < 0 || r >= nrows_sumw || ic < 0 || ic >= nchan_img) { raise_error(err, YG_ERR_CINDEX, s); continue; }
-    for (int p = 0; p < v.npol; ++p) {
-      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
-      const float wt = noise_weight(nre);
-      if (!(wt > 0.f)) { raise_error(err, YG_ERR_WEIGHT, s); continue; }
-      atomicAdd(&sumw[r + (long long)nrows_sumw * (p + (long long)v.npol * ic)], (double)wt);
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // k_grid
 // ---------------------------------------------------------------------------
@@ -325,7 +302,7 @@ __host__ __device__ __forceinline__ unsigned cf_bytes(int w) { return (unsigned)
 // of one row, so its CF taps and grid cells fall on 16 distinct banks (Wp and
 // the CF row stride are multiples of 16).  Taps of the padding are exact zeros
 // and land in the tile's gutter (columns/rows >= P), which is never read back.
-template <int NPOL, int MAXSLOTS>
+template <int NPOL, int MAXSLOTS, int RSTEP>
 __global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int Pg = a.Pg;
@@ -369,15 +346,27 @@ __global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
     if (e0 < it.z) issue(e0, 1);
   }
 
-  int rx[MAXSLOTS], rowoff[MAXSLOTS];
-  bool live[MAXSLOTS];
+  // RSTEP == 0: slot q of thread t owns residue k = q * blockDim + t.
+  // RSTEP > 0 (blockDim = RSTEP * Wp, MAXSLOTS * RSTEP = Wp): thread t owns
+  // the x residue t mod Wp and the y residues t / Wp + RSTEP * q, so the x
+  // part of the index arithmetic is done once per sample and the slots step
+  // down the rows.
+  int rx[RSTEP ? 1 : MAXSLOTS], rowoff[RSTEP ? 1 : MAXSLOTS];
+  bool live[RSTEP ? 1 : MAXSLOTS];
+  if (RSTEP) {
+    rx[0] = threadIdx.x % Wp;
+    rowoff[0] = threadIdx.x / Wp;
+    live[0] = true;
+  } else {
 #pragma unroll
-  for (int q = 0; q < MAXSLOTS; ++q) {
-    const int k = q * blockDim.x + threadIdx.x;
-    live[q] = k < Wp2;
-    rx[q] = live[q] ? k % Wp : 0;
-    rowoff[q] = live[q] ? k / Wp : 0;   // ry
+    for (int q = 0; q < (RSTEP ? 1 : MAXSLOTS); ++q) {
+      const int k = q * blockDim.x + threadIdx.x;
+      live[q] = k < Wp2;
+      rx[q] = live[q] ? k % Wp : 0;
+      rowoff[q] = live[q] ? k / Wp : 0;   // ry
+    }
   }
+  const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
 
   unsigned fphase[2] = {0u, 0u}, ephase[2] = {0u, 0u};
   bool ok = true;
@@ -407,6 +396,31 @@ __global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
       const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
       const int cb = px0 + Pg * py0;
       const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
+      if (RSTEP) {
+        int jx = rx[0] - mx;
+        jx += (jx < 0) ? Wp : 0;
+        int jy0 = rowoff[0] - my;
+        jy0 += (jy0 < 0) ? Wp : 0;
+        int cell = cb + jx + Pg * jy0;
+        int tap = jx + Wp * jy0;
+        const int lim = Wp - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
+#pragma unroll
+        for (int q = 0; q < MAXSLOTS; ++q) {
+          const bool wrap = RSTEP * q >= lim;
+          const int c2 = wrap ? cell - PgW : cell;
+          const int t2 = wrap ? tap - Wp2 : tap;
+          const float2 c = cf_s[t2];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            float2 g = acc_s[p * PG2 + c2];
+            g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
+            g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
+            acc_s[p * PG2 + c2] = g;
+          }
+          cell += PgR;
+          tap += WpR;
+        }
+      } else {
 #pragma unroll
       for (int q = 0; q < MAXSLOTS; ++q) {
         int jx = rx[q] - mx;
@@ -422,6 +436,7 @@ __global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
           g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
           acc_s[p * PG2 + cell] = g;
         }
+      }
       }
       r = rn;
 #pragma unroll
@@ -491,32 +506,80 @@ __global__ void k_records(const unsigned int* __restrict__ val, const unsigned i
 
 // Per sorted sample, once per grid pass: rVis = phasor * conj(vis) * wt (* mfs)
 // (TableVisGridder.cc:775-806), or wt (* mfs) for the PSF.
-__global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long nvalid, float2* __restrict__ out) {
+// Gathers the weighted visibilities of the sorted samples (phase rotation,
+// conjugation, weight and MFS factor of TableVisGridder::generic) and adds the
+// weights into the sums of weights, in double, per (CF row, pol, image channel)
+// (TableVisGridder.cc:783-823).  The records are sorted by tile and CF index,
+// so neighbouring samples mostly share one sum-of-weights row: a segmented
+// warp scan adds each run of equal rows once, one atomic per polarisation,
+// instead of one per sample.
+__global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long nvalid, float2* __restrict__ out,
+                             SumwArgs sw, DevError* err) {
   const long long n = v.nrow * (long long)v.nchan;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
-    const long long s = rec[i].w;
-    const long long row = s % v.nrow;
-    const int chan = (int)(s / v.nrow);
-    float pr, pi;
-    phasor_of(v, row, chan, &pr, &pi);
-    const float m = v.mfs ? v.mfs[chan] : 1.f;
-    for (int p = 0; p < v.npol; ++p) {
-      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
-      const float wt = noise_weight(nre);
-      float2 o;
-      if (v.psf) {
-        o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
-        o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
-      } else {
-        const float2 vv = v.vis[s + n * p];
-        const float vr = vv.x, vi = -vv.y;
-        float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
-        float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
-        rr = __fmul_rn(__fmul_rn(rr, wt), m);
-        ri = __fmul_rn(__fmul_rn(ri, wt), m);
-        o = make_float2(rr, ri);
+  const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = blockIdx.x * (long long)blockDim.x + threadIdx.x - lane; base < nvalid; base += stride) {
+    const long long i = base + lane;
+    long long bin = -1;
+    float wts[4] = {0.f, 0.f, 0.f, 0.f};
+    if (i < nvalid) {
+      const int4 r = rec[i];
+      const long long s = r.w;
+      const long long row = s % v.nrow;
+      const int chan = (int)(s / v.nrow);
+      float pr, pi;
+      phasor_of(v, row, chan, &pr, &pi);
+      const float m = v.mfs ? v.mfs[chan] : 1.f;
+      bool good = true;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        if (p >= v.npol) break;
+        const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
+        const float wt = noise_weight(nre);
+        if (!(wt > 0.f)) good = false;
+        wts[p] = wt;
+        float2 o;
+        if (v.psf) {
+          o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
+          o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
+        } else {
+          const float2 vv = v.vis[s + n * p];
+          const float vr = vv.x, vi = -vv.y;
+          float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+          float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+          rr = __fmul_rn(__fmul_rn(rr, wt), m);
+          ri = __fmul_rn(__fmul_rn(ri, wt), m);
+          o = make_float2(rr, ri);
+        }
+        out[(size_t)i * v.npol + p] = o;
       }
-      out[(size_t)i * v.npol + p] = o;
+      if (!good) raise_error(err, YG_ERR_WEIGHT, s);
+      if (sw.sumw && good) {
+        const int rr = sw.track_per_os ? r.z : r.z / (sw.os * sw.os);
+        const int ic = sw.chan_map[chan];
+        if (rr < 0 || rr >= sw.nrows || ic < 0 || ic >= sw.nchan_img) {
+          raise_error(err, YG_ERR_CINDEX, s);
+        } else {
+          bin = rr + (long long)sw.nrows * v.npol * ic;
+        }
+      }
+    }
+    if (!sw.sumw) continue;    // uniform over the grid: no lane is left out of the shuffles
+    const long long prev = __shfl_up_sync(full, bin, 1);
+    const unsigned heads = __ballot_sync(full, lane == 0 || prev != bin);
+    const int seg0 = 31 - __clz(heads & (full >> (31 - lane)));
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      if (p >= v.npol) break;
+      double x = bin >= 0 ? (double)wts[p] : 0.0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double y = __shfl_up_sync(full, x, off);
+        if (lane - off >= seg0) x += y;
+      }
+      if (tail && bin >= 0) atomicAdd(&sw.sumw[bin + (long long)sw.nrows * p], x);
     }
   }
 }
@@ -751,6 +814,193 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
   }
 }
 
+// Degridding of one work item on the padded layout: the grid tile (stride Pg,
+// zero outside the grid) is staged in shared memory, and the CF plane of each
+// run of equal-CF samples is brought in by a TMA bulk copy two runs ahead
+// (full/empty mbarriers, producer thread 0).  One warp per sample walks the
+// Wp x Wp taps 32 at a time: a half-warp reads 16 consecutive taps of one row,
+// so CF and grid reads fall on distinct banks; padded taps are exact zeros.
+// Four partial sums per lane hide the FMA latency; a warp shuffle combines
+// them (GridKernel.cc:99-137).
+struct DegridTArgs {
+  const int4* items;
+  const int4* rec;
+  const int* runend;
+  VisArgs v;
+  CFView cf;
+  const float2* grid;
+  int nx, ny, nchan_img;
+  int tile, ntx;
+  long long ntiles;
+  int smax, Pg, Wp, cfbuf;
+  float2* out;
+  DevError* err;
+};
+
+template <int NPOL>
+__global__ void __launch_bounds__(kDegridThreads) k_degrid_t(DegridTArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int Pg = a.Pg, PG2 = Pg * Pg;
+  const int Wp = a.Wp, Wp2 = Wp * Wp;
+  float2* g_s = reinterpret_cast<float2*>(smem_raw);
+  unsigned char* cfb = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
+  cfb = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(cfb) + 127) & ~(size_t)127);
+  float2* cfs[2] = {reinterpret_cast<float2*>(cfb), reinterpret_cast<float2*>(cfb + a.cfbuf)};
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(cfb + 2 * (size_t)a.cfbuf);
+  unsigned long long* empty = full + 2;
+  __shared__ int s_abort;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+
+  const int4 it = a.items[blockIdx.x];
+  const long long gc = (long long)it.x / a.ntiles;
+  const long long t = (long long)it.x % a.ntiles;
+  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
+  const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
+  const int gind = (int)(gc / a.nchan_img), ichan = (int)(gc % a.nchan_img);
+  const long long plane_cells = (long long)a.nx * a.ny;
+  const float2* gbase = a.grid + (size_t)gind * plane_cells * NPOL * a.nchan_img + plane_cells * ((size_t)NPOL * ichan);
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], nwarps);
+    mbar_init(&empty[1], nwarps);
+    mbar_fence_init();
+  }
+  const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
+  auto run_end = [&](int j) { return max(j + 1, min(a.runend[j], it.z)); };
+  auto issue = [&](int start, int buf) {
+    const int c = a.rec[start].z;
+    mbar_expect_tx(&full[buf], cfcopy);
+    bulk_g2s(cfs[buf], a.cf.pad + (size_t)c * Wp2, cfcopy, &full[buf]);
+  };
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    issue(it.y, 0);
+    const int e0 = run_end(it.y);
+    if (e0 < it.z) issue(e0, 1);
+  }
+  for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) {
+    const int p = i / PG2, c = i % PG2;
+    const int x = X0 + c % Pg, y = Y0 + c / Pg;
+    float2 g = make_float2(0.f, 0.f);
+    if (x >= 0 && y >= 0 && x < a.nx && y < a.ny) g = gbase[plane_cells * p + x + (size_t)a.nx * y];
+    g_s[i] = g;
+  }
+  __syncthreads();
+
+  // lane's first tap and its grid-cell offset inside the footprint
+  const int jx0 = lane % Wp, jy0 = lane / Wp;
+  const int steps = Wp2 / 32;        // Wp is a multiple of 16: Wp^2 / 32 is a multiple of 8
+  const int rows_per_step = 32 / Wp; // 2 when Wp == 16, else 0 (wrap handled below)
+  unsigned fphase[2] = {0u, 0u}, ephase[2] = {0u, 0u};
+  bool ok = true;
+  int b = 0;
+  for (int j = it.y; j < it.z;) {
+    const int e = run_end(j);
+    if (!mbar_wait(&full[b], fphase[b])) {
+      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+      ok = false;
+      break;
+    }
+    fphase[b] ^= 1u;
+    const float2* __restrict__ cf_s = cfs[b];
+    for (int i = j + warp; i < e; i += nwarps) {
+      const int4 r = a.rec[i];
+      const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
+      const int origin = px0 + Pg * py0;
+      float re[4][NPOL], im[4][NPOL];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) re[u][p] = im[u][p] = 0.f;
+      int tap = lane;
+      int jx = jx0;
+      int cell = origin + jx0 + Pg * jy0;
+      for (int st = 0; st < steps; st += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float2 cv = cf_s[tap];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            const float2 g = g_s[p * PG2 + cell];
+            re[u][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[u][p]));
+            im[u][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[u][p]));
+          }
+          tap += 32;
+          if (rows_per_step) {
+            cell += rows_per_step * Pg;
+          } else {
+            jx += 32;
+            const bool wrap = jx >= Wp;
+            jx = wrap ? jx - Wp : jx;
+            cell += wrap ? 32 - Wp + Pg : 32;
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
+        float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          sr += __shfl_xor_sync(0xffffffffu, sr, off);
+          si += __shfl_xor_sync(0xffffffffu, si, off);
+        }
+        re[0][p] = sr;
+        im[0][p] = si;
+      }
+      if (lane == 0) {
+        const long long s = r.w;
+        const long long row = s % a.v.nrow;
+        const int chan = (int)(s / a.v.nrow);
+        float pr, pi;
+        phasor_of(a.v, row, chan, &pr, &pi);
+        const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          float cr = re[0][p], ci = im[0][p];
+          if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
+          a.out[(size_t)s * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
+                                                    __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
+    if (threadIdx.x == 0 && e < it.z) {
+      const int e2 = run_end(e);
+      if (e2 < it.z) {
+        if (!mbar_wait(&empty[b], ephase[b])) {
+          raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+          s_abort = 1;
+        } else {
+          fence_proxy_async_smem();
+          issue(e2, b);
+        }
+      }
+    }
+    ephase[b] ^= 1u;
+    j = e;
+    b ^= 1;
+    if (s_abort) {
+      ok = false;
+      break;
+    }
+  }
+  if (!ok && threadIdx.x == 0) {
+    mbar_wait(&full[0], fphase[0]);
+    mbar_wait(&full[1], fphase[1]);
+  }
+}
+
+size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf) {
+  return (size_t)npol * Pg * Pg * sizeof(float2) + 128 + 2 * (size_t)cfbuf + 4 * sizeof(unsigned long long);
+}
+
 // prev[o] = o when sample (row, chan) with o = row * nchan + chan is on-grid,
 // -1 otherwise (input of the max-scan)
 __global__ void k_order_marks(const unsigned char* __restrict__ status, long long nrow, int nchan, int want,
@@ -770,22 +1020,21 @@ __global__ void k_order_marks(const unsigned char* __restrict__ status, long lon
 __global__ void k_degrid_writeback(const unsigned char* __restrict__ status, const int* __restrict__ prev,
                                    const float2* __restrict__ vals, const float2* __restrict__ carry,
                                    long long nrow, int nchan, int npol, float2* __restrict__ vis) {
+  // sample order s = row + nrow * chan: the cube's own order, so the
+  // read-modify-write of vis and the reads of vals are coalesced; only
+  // off-grid samples (status 2) look up their loop-order predecessor
   const long long n = nrow * (long long)nchan;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
-    const long long row = o / nchan;
-    const int chan = (int)(o % nchan);
-    const long long s = row + nrow * chan;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const unsigned char st = status[s];
     if (st < 2) continue;
-    const int q = prev[o];
+    long long src = s;
+    if (st != 3) {
+      const long long o = (s % nrow) * nchan + s / nrow;
+      const int q = prev[o];
+      src = q >= 0 ? (q / nchan) + nrow * (q % nchan) : -1;
+    }
     for (int p = 0; p < npol; ++p) {
-      float2 v;
-      if (q >= 0) {
-        const long long sq = (q / nchan) + nrow * (q % nchan);
-        v = vals[(size_t)sq * npol + p];
-      } else {
-        v = carry[p];
-      }
+      const float2 v = src >= 0 ? vals[(size_t)src * npol + p] : carry[p];
       float2 o2 = vis[s + n * p];
       o2.x += v.x;
       o2.y += v.y;
@@ -794,12 +1043,26 @@ __global__ void k_degrid_writeback(const unsigned char* __restrict__ status, con
   }
 }
 
-// carry_out = value of the last sample in loop order with status >= want
-__global__ void k_update_carry(const int* __restrict__ prev, long long nrow, int nchan, int npol,
+// *last = the largest loop-order index o = row * nchan + chan whose sample has
+// status >= want (stays -1 when there is none); *last must be -1 on entry
+__global__ void k_last_marked(const unsigned char* __restrict__ status, long long nrow, int nchan, int want,
+                              int* __restrict__ last) {
+  const long long n = nrow * (long long)nchan;
+  int best = -1;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+    if (status[s] >= want) best = max(best, (int)((s % nrow) * nchan + s / nrow));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
+  if ((threadIdx.x & 31) == 0 && best >= 0) atomicMax(last, best);
+}
+
+// carry_out = value of the sample with loop-order index *q (unchanged if q < 0)
+__global__ void k_update_carry(const int* __restrict__ qp, long long nrow, int nchan, int npol,
                                const float2* __restrict__ vals, int vals_are_vis, float2* __restrict__ carry) {
   const long long n = nrow * (long long)nchan;
   if (n == 0) return;
-  const int q = prev[n - 1];
+  const int q = *qp;
   if (q < 0) return;
   const long long sq = (q / nchan) + nrow * (q % nchan);
   for (int p = threadIdx.x; p < npol; p += blockDim.x) {
@@ -833,6 +1096,7 @@ static int ceil_log2(unsigned long long v) {
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st) {
   const long long n = a.nrow * (long long)a.nchan;
   pl.nsamples = n;
+  pl.prev_ready = false;
   pl.nrow = a.nrow;
   pl.nchan = a.nchan;
   pl.npol = a.npol;
@@ -942,25 +1206,37 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
 }
 
 
-template <int NPOL, int MAXSLOTS>
+template <int NPOL, int MAXSLOTS, int RSTEP>
 static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
-  auto k = k_grid<NPOL, MAXSLOTS>;
+  auto k = k_grid<NPOL, MAXSLOTS, RSTEP>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<nitems, threads, smem, st>>>(g);
   YG_COUNT_LAUNCH();
   return cudaGetLastError();
 }
 
-// threads x slots covering Wp^2 residue classes with the least waste
-// (threads a multiple of 32, at most 512)
+// threads x slots covering Wp^2 residue classes: the row layout where one
+// exists for Wp, else the least-waste generic layout (threads a multiple of
+// 32, at most 512)
 struct GridShape {
-  int threads, slots;
+  int threads, slots, rstep;
 };
 
 GridShape grid_shape(int Wp) {
+  switch (Wp) {
+    case 16: return GridShape{256, 1, 16};
+    case 32: return GridShape{256, 4, 8};
+    case 48: return GridShape{384, 6, 8};
+    case 64: return GridShape{512, 8, 8};
+    case 80: return GridShape{320, 20, 4};
+    case 96: return GridShape{384, 24, 4};
+    case 112: return GridShape{448, 28, 4};
+    case 128: return GridShape{512, 32, 4};
+    default: break;
+  }
   const int W2 = Wp * Wp;
   const int cand[10] = {1, 2, 3, 4, 6, 8, 9, 12, 16, 25};
-  GridShape best{0, 0};
+  GridShape best{0, 0, 0};
   long long best_waste = -1;
   for (int sl : cand) {
     int th = ((W2 + sl - 1) / sl + 31) / 32 * 32;
@@ -968,7 +1244,7 @@ GridShape grid_shape(int Wp) {
     if (th > 512) continue;
     const long long waste = (long long)th * sl - W2;
     if (best_waste < 0 || waste < best_waste || (waste == best_waste && th > best.threads)) {
-      best = GridShape{th, sl};
+      best = GridShape{th, sl, 0};
       best_waste = waste;
     }
   }
@@ -978,17 +1254,30 @@ GridShape grid_shape(int Wp) {
 template <int NPOL>
 static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, GridShape sh, cudaStream_t st) {
   const int t = sh.threads;
+  if (sh.rstep) {
+    switch (sh.slots * 1000 + sh.rstep) {
+      case 1016: return launch_grid_ms<NPOL, 1, 16>(g, nitems, t, smem, st);
+      case 4008: return launch_grid_ms<NPOL, 4, 8>(g, nitems, t, smem, st);
+      case 6008: return launch_grid_ms<NPOL, 6, 8>(g, nitems, t, smem, st);
+      case 8008: return launch_grid_ms<NPOL, 8, 8>(g, nitems, t, smem, st);
+      case 20004: return launch_grid_ms<NPOL, 20, 4>(g, nitems, t, smem, st);
+      case 24004: return launch_grid_ms<NPOL, 24, 4>(g, nitems, t, smem, st);
+      case 28004: return launch_grid_ms<NPOL, 28, 4>(g, nitems, t, smem, st);
+      case 32004: return launch_grid_ms<NPOL, 32, 4>(g, nitems, t, smem, st);
+      default: return cudaErrorInvalidConfiguration;
+    }
+  }
   switch (sh.slots) {
-    case 1: return launch_grid_ms<NPOL, 1>(g, nitems, t, smem, st);
-    case 2: return launch_grid_ms<NPOL, 2>(g, nitems, t, smem, st);
-    case 3: return launch_grid_ms<NPOL, 3>(g, nitems, t, smem, st);
-    case 4: return launch_grid_ms<NPOL, 4>(g, nitems, t, smem, st);
-    case 6: return launch_grid_ms<NPOL, 6>(g, nitems, t, smem, st);
-    case 8: return launch_grid_ms<NPOL, 8>(g, nitems, t, smem, st);
-    case 9: return launch_grid_ms<NPOL, 9>(g, nitems, t, smem, st);
-    case 12: return launch_grid_ms<NPOL, 12>(g, nitems, t, smem, st);
-    case 16: return launch_grid_ms<NPOL, 16>(g, nitems, t, smem, st);
-    case 25: return launch_grid_ms<NPOL, 25>(g, nitems, t, smem, st);
+    case 1: return launch_grid_ms<NPOL, 1, 0>(g, nitems, t, smem, st);
+    case 2: return launch_grid_ms<NPOL, 2, 0>(g, nitems, t, smem, st);
+    case 3: return launch_grid_ms<NPOL, 3, 0>(g, nitems, t, smem, st);
+    case 4: return launch_grid_ms<NPOL, 4, 0>(g, nitems, t, smem, st);
+    case 6: return launch_grid_ms<NPOL, 6, 0>(g, nitems, t, smem, st);
+    case 8: return launch_grid_ms<NPOL, 8, 0>(g, nitems, t, smem, st);
+    case 9: return launch_grid_ms<NPOL, 9, 0>(g, nitems, t, smem, st);
+    case 12: return launch_grid_ms<NPOL, 12, 0>(g, nitems, t, smem, st);
+    case 16: return launch_grid_ms<NPOL, 16, 0>(g, nitems, t, smem, st);
+    case 25: return launch_grid_ms<NPOL, 25, 0>(g, nitems, t, smem, st);
     default: break;
   }
   return cudaErrorInvalidConfiguration;
@@ -1018,8 +1307,8 @@ int grid_pols_per_pass(int npol, int Pg, int cfbuf) {
 
 // Grids the samples of a plan onto `grid` (ngrid planes of (nx, ny, npol, nchan_img)).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
-              DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
-              int mode) {
+              const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0,
+              cudaEvent_t ev1, int mode) {
   (void)mode;
   if (pl.nitems == 0) return YG_OK;
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
@@ -1030,7 +1319,8 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
   YG_CUDA_TRY(svis.ensure((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
-  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>());
+  if (v.npol > 4) return YG_ERR_UNSUPPORTED;
+  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>(), sw, err);
   YG_COUNT_LAUNCH();
   GridKArgs g;
   g.items = pl.items.as<int4>();
@@ -1092,16 +1382,6 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   return YG_OK;
 }
 
-int plan_sumw(const Plan& pl, const VisArgs& v, const int* chan_map, int os, int track_per_os, int nrows_sumw,
-              int nchan_img, double* sumw, DevError* err, cudaStream_t st) {
-  if (pl.nsamples == 0) return YG_OK;
-  k_sumw<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, pl.status.as<unsigned char>(), pl.cfi.as<int>(), chan_map,
-                                                     os, track_per_os, nrows_sumw, nchan_img, sumw, err);
-  YG_COUNT_LAUNCH();
-  YG_CUDA_TRY(cudaGetLastError());
-  return YG_OK;
-}
-
 // Degrids the samples of a plan from `grid` and adds the result into vis.
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
@@ -1109,7 +1389,47 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
-  if (pl.nitems > 0) {
+  bool done = false;
+  if (pl.nitems > 0 && cf.pad && cf.wpad > 0 && cf.wpad <= 128 && (v.npol == 1 || v.npol == 2 || v.npol == 4)) {
+    DegridTArgs d;
+    d.items = pl.items.as<int4>();
+    d.rec = pl.rec.as<int4>();
+    d.runend = pl.runend.as<int>();
+    d.v = v;
+    d.cf = cf;
+    d.grid = grid;
+    d.nx = nx;
+    d.ny = ny;
+    d.nchan_img = nchan_img;
+    d.tile = pl.tile;
+    d.ntx = pl.ntx;
+    d.ntiles = (long long)pl.ntx * pl.nty;
+    d.smax = pl.smax;
+    d.Pg = grid_tile_stride(pl.tile, cf.wpad, pl.smax, cf.varsup != 0);
+    d.Wp = cf.wpad;
+    d.cfbuf = grid_cf_buffer_bytes(cf.wpad);
+    d.out = tmp_vals.as<float2>();
+    d.err = err;
+    const size_t smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf);
+    if (smem <= 227 * 1024) {
+      if (ev0) cudaEventRecord(ev0, st);
+      if (v.npol == 1) {
+        cudaFuncSetAttribute(k_degrid_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_degrid_t<1><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+      } else if (v.npol == 2) {
+        cudaFuncSetAttribute(k_degrid_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_degrid_t<2><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+      } else {
+        cudaFuncSetAttribute(k_degrid_t<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_degrid_t<4><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+      }
+      YG_COUNT_LAUNCH();
+      if (ev1) cudaEventRecord(ev1, st);
+      YG_CUDA_TRY(cudaGetLastError());
+      done = true;
+    }
+  }
+  if (pl.nitems > 0 && !done) {
     DegridKArgs d;
     d.items = pl.items.as<int4>();
     d.rec = pl.rec.as<int4>();
@@ -1166,20 +1486,25 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     e = cudaGetLastError();
     if (e != cudaSuccess) return YG_ERR_CUDA;
   }
-  // write-back with the reference's carried value for off-grid samples
+  // write-back with the reference's carried value for off-grid samples; the
+  // loop-order predecessor scan depends only on the plan, so it is computed
+  // on the first degridding pass of a plan and kept
   YG_CUDA_TRY(pl.order_prev.ensure((size_t)n * 4 * 2));
   int* marks = pl.order_prev.as<int>();
   int* prev = marks + n;
-  k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 3, marks);
-  YG_COUNT_LAUNCH();
-  size_t tmp = 0;
-  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
-  YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
-  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
+  if (!pl.prev_ready) {
+    k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 3, marks);
+    YG_COUNT_LAUNCH();
+    size_t tmp = 0;
+    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
+    YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
+    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
+    pl.prev_ready = true;
+  }
   k_degrid_writeback<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), prev, tmp_vals.as<float2>(),
                                                        carry, pl.nrow, pl.nchan, v.npol, vis_out);
   YG_COUNT_LAUNCH();
-  k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, tmp_vals.as<float2>(), 0, carry);
+  k_update_carry<<<1, 32, 0, st>>>(prev + (n - 1), pl.nrow, pl.nchan, v.npol, tmp_vals.as<float2>(), 0, carry);
   YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
@@ -1190,16 +1515,12 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st) {
   const long long n = pl.nsamples;
   if (n == 0 || v.psf) return YG_OK;
-  YG_CUDA_TRY(pl.order_prev.ensure((size_t)n * 4 * 2));
-  int* marks = pl.order_prev.as<int>();
-  int* prev = marks + n;
-  k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 1, marks);
+  YG_CUDA_TRY(pl.last.ensure(sizeof(int)));
+  YG_CUDA_TRY(cudaMemsetAsync(pl.last.p, 0xff, sizeof(int), st));
+  k_last_marked<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 1,
+                                                  pl.last.as<int>());
   YG_COUNT_LAUNCH();
-  size_t tmp = 0;
-  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
-  YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
-  YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
-  k_update_carry<<<1, 32, 0, st>>>(prev, pl.nrow, pl.nchan, v.npol, v.vis, 1, carry);
+  k_update_carry<<<1, 32, 0, st>>>(pl.last.as<int>(), pl.nrow, pl.nchan, v.npol, v.vis, 1, carry);
   YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;

@@ -102,7 +102,9 @@ struct Plan {
   int nchan = 0, npol = 0;
   DevBuf key, key_alt, val, val_alt, pos, cfi, status;
   DevBuf tstart, tend, nit, itembase, items, nvalid_d, sort_tmp;
-  DevBuf order_prev;            // degrid stale-value scan
+  DevBuf order_prev;            // degrid stale-value scan: marks, then loop-order predecessors
+  bool prev_ready = false;      // order_prev holds this plan's predecessors
+  DevBuf last;                  // grid carry: loop-order index of the last used sample
   DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
   DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
   DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
@@ -121,6 +123,15 @@ struct VisArgs {
   int npol;
   int psf;                  // grid the weight instead of the visibility
   const uint8_t* psf_ok;    // nrow representative feed/field mask (PSF), may be null
+};
+
+// Sums of weights (rows, npol, image channels), column-major, in double; rows
+// are CF planes (or CF indices when the weight is tracked per oversampling
+// plane).  sumw == nullptr: not accumulated.
+struct SumwArgs {
+  double* sumw;
+  const int* chan_map;
+  int os, track_per_os, nrows, nchan_img;
 };
 
 }  // namespace yg
