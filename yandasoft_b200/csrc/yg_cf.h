@@ -71,9 +71,8 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
                 cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
-size_t grid_smem_bytes(int npol, int Pg, int cfbuf);
-int grid_pols_per_pass(int npol, int Pg, int cfbuf);
 int grid_cf_buffer_bytes(int wpad);
+int grid_tile_for(int smax, int npol, bool varsup);
 int grid_tile_stride(int tile, int wpad, int smax, bool varsup);
 extern std::atomic<long long> g_kernel_launches;
 

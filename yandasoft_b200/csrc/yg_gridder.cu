@@ -700,26 +700,7 @@ void Gridder::init_cf(const Chunk& dc) {
 // ---------------------------------------------------------------------------
 int Gridder::tile_for(int smax, int npol) const {
   if (tile_override_ > 0) return tile_override_;
-  // largest multiple of 8 whose guttered tile and two padded CF buffers fit
-  // ~110 KB of shared memory for the polarisations accumulated per pass (two
-  // CTAs per SM), else 220 KB (one CTA per SM)
-  const int wpad = ((2 * smax + 1) + 15) / 16 * 16;
-  const bool varsup = cf_.view().varsup != 0;
-  const int cfbuf = grid_cf_buffer_bytes(wpad);
-  const int budgets[2] = {110 * 1024, 220 * 1024};
-  for (int b : budgets) {
-    for (int npa : {npol, 2, 1}) {
-      if (npa > npol || npol % npa) continue;
-      const double rest = (double)b - 2.0 * cfbuf - 256.0;
-      if (rest <= 0) continue;
-      const double pg2 = rest / (8.0 * npa) - 512.0;
-      if (pg2 <= 0) continue;
-      const int pgmax = (int)std::sqrt(pg2);
-      const int t = (pgmax - (wpad - 1) - (varsup ? smax : 0)) / 8 * 8;
-      if (t >= 32) return std::min(t, 256);
-    }
-  }
-  return 16;
+  return grid_tile_for(smax, npol, cf_.view().varsup != 0);
 }
 
 void Gridder::fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, const uint8_t* row_ok) const {

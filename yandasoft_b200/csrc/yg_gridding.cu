@@ -235,6 +235,8 @@ struct GridKArgs {
   float2* scratch;           // [item][npol][P][P]
   int pol0;                  // first polarisation of this pass
   int npol_total;            // polarisations of the visibility cube
+  int stage_bytes;           // bytes of one segment stage
+  int nstages;               // depth of the segment ring
   DevError* err;
 };
 
@@ -289,193 +291,263 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phas
 
 __host__ __device__ __forceinline__ unsigned cf_bytes(int w) { return (unsigned)(((w * w * 8) + 15) & ~15); }
 
-// Gridding of one work item.  CF planes are shared by runs of consecutive
-// samples (the sort key orders samples by CF inside a tile); each run's plane,
-// zero-padded to Wp x Wp with Wp = round_up(2 Smax + 1, 16), is brought into
-// shared memory by a TMA bulk copy two runs ahead, with full/empty mbarriers
-// between the copy (issued by thread 0) and the warps, so warps never meet at
-// a CTA-wide barrier inside the item.
+// Ring of segment stages shared by the producer warp and the tap warps of
+// k_grid and k_degrid_t.  A segment is up to kSeg consecutive sorted samples
+// of one run (same tile and CF); its stage holds the CF plane (zero-padded to
+// Wp x Wp, brought in by a TMA bulk copy), the samples' records and
+// visibilities, and a header {count, index of the segment's first sample in
+// the item}.  count < 0 marks the end of the item.
+constexpr int kSeg = 32;
+
+__host__ __device__ __forceinline__ int seg_stage_bytes(int cfbuf, int npol) {
+  return (cfbuf + kSeg * 16 + kSeg * npol * 8 + 16 + 127) / 128 * 128;
+}
+
+// Fewest stages worth keeping two CTAs per SM for: small CF planes come with
+// short runs (a segment per sample or so), so the ring must run several
+// segments ahead; large ones carry many taps per segment, so two suffice.
+static int min_stages_two_ctas(size_t stage) { return stage >= 8192 ? 2 : 4; }
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Producer warp: walks the item's sorted samples 32 at a time (records and
+// visibilities loaded one window ahead), cuts each window at CF changes and
+// fills one stage per segment.  Returns false when a wait on a stage gave up.
+template <int NV>
+__device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restrict__ rec,
+                                            const float2* __restrict__ vis, int vis_stride, int vis_off,
+                                            const float2* __restrict__ cfpad, int Wp2, int cfbuf, int SB, int NST,
+                                            unsigned char* ring, unsigned long long* full,
+                                            unsigned long long* empty, int& seg) {
+  const int lane = threadIdx.x & 31;
+  const unsigned fm = 0xffffffffu;
+  const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
+  seg = 0;
+  auto load = [&](int base, int4& r, float2 (&v)[NV > 0 ? NV : 1]) {
+    const int i = base + lane;
+    if (i < it.z) {
+      r = rec[i];
+#pragma unroll
+      for (int p = 0; p < NV; ++p) v[p] = vis[(size_t)i * vis_stride + vis_off + p];
+    } else {
+      r = make_int4(0, 0, -1, -1);
+    }
+  };
+  auto acquire = [&](int stage) -> bool {
+    bool okw = true;
+    if (seg >= NST && lane == 0) okw = mbar_wait(&empty[stage], (unsigned)((seg / NST) - 1) & 1u);
+    return __shfl_sync(fm, okw ? 1 : 0, 0) != 0;
+  };
+  int4 r;
+  float2 v[NV > 0 ? NV : 1];
+  load(it.y, r, v);
+  for (int base = it.y; base < it.z; base += 32) {
+    int4 rn;
+    float2 vn[NV > 0 ? NV : 1];
+    load(base + 32, rn, vn);                       // next window in flight
+    const int nwin = min(32, it.z - base);
+    const int zprev = __shfl_up_sync(fm, r.z, 1);
+    unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || zprev != r.z));
+    while (heads) {
+      const int h = __ffs(heads) - 1;
+      heads &= heads - 1;
+      const int h2 = heads ? __ffs(heads) - 1 : nwin;
+      const int stage = seg % NST;
+      if (!acquire(stage)) return false;
+      unsigned char* sp = ring + (size_t)stage * SB;
+      if (lane >= h && lane < h2) {
+        reinterpret_cast<int4*>(sp + cfbuf)[lane - h] = r;
+        float2* vs = reinterpret_cast<float2*>(sp + cfbuf + kSeg * 16);
+#pragma unroll
+        for (int p = 0; p < NV; ++p) vs[(lane - h) * NV + p] = v[p];
+      }
+      const int cfi = __shfl_sync(fm, r.z, h);
+      if (lane == 0) {
+        int* hdr = reinterpret_cast<int*>(sp + SB - 16);
+        hdr[0] = h2 - h;
+        hdr[1] = base + h - it.y;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        fence_proxy_async_smem();
+        mbar_expect_tx(&full[stage], cfcopy);
+        bulk_g2s(sp, cfpad + (size_t)cfi * Wp2, cfcopy, &full[stage]);
+      }
+      ++seg;
+    }
+    r = rn;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) v[p] = vn[p];
+  }
+  const int stage = seg % NST;
+  if (!acquire(stage)) return false;
+  if (lane == 0) {
+    reinterpret_cast<int*>(ring + (size_t)stage * SB + SB - 16)[0] = -1;
+    mbar_arrive(&full[stage]);
+  }
+  ++seg;
+  return true;
+}
+
+// After a failed wait: the producer's lane 0 waits (bounded) until the last
+// fill of every stage has landed, so no copy is in flight when the CTA exits.
+__device__ __forceinline__ void seg_drain(int nfill, int NST, unsigned long long* full) {
+  for (int q = 0; q < NST && q < nfill; ++q) {
+    const int nq = (nfill - q + NST - 1) / NST;   // fills of stage q
+    mbar_wait(&full[q], (unsigned)(nq - 1) & 1u);
+  }
+}
+
+// Gridding of one work item.  Thread/slot k of the tap warps owns the cells
+// with (x mod Wp, y mod Wp) = (k mod Wp, k / Wp): no two threads touch the
+// same cell, so every tap is accumulated in place in shared memory without
+// atomics.  A half-warp holds 16 consecutive residues of one row, so its CF
+// taps and grid cells fall on 16 distinct banks (Wp and the CF row stride are
+// multiples of 16).  Taps of the padding are exact zeros and land in the
+// tile's gutter (columns/rows >= P), which is never read back.
 //
-// Thread/slot k owns the cells with (x mod Wp, y mod Wp) = (k mod Wp, k / Wp):
-// no two threads touch the same cell, so every tap is accumulated in place in
-// shared memory without atomics.  A half-warp holds 16 consecutive residues
-// of one row, so its CF taps and grid cells fall on 16 distinct banks (Wp and
-// the CF row stride are multiples of 16).  Taps of the padding are exact zeros
-// and land in the tile's gutter (columns/rows >= P), which is never read back.
+// The last warp is the producer: it stages segments (CF plane by TMA, records
+// and visibilities by the warp) into an NST-deep ring with full/empty
+// mbarriers, so the tap warps read nothing but shared memory and never wait
+// on a global load.
 template <int NPOL, int MAXSLOTS, int RSTEP>
-__global__ void __launch_bounds__(512) k_grid(GridKArgs a) {
+__global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nthr = blockDim.x - 32;              // tap threads
+  const int ncw = nthr / 32;
   const int Pg = a.Pg;
-  const int PG2 = Pg * Pg + (int)blockDim.x;   // per polarisation: tile + one trash cell per thread
+  const int PG2 = Pg * Pg + nthr;                // per polarisation: tile + one trash cell per tap thread
   float2* acc_s = reinterpret_cast<float2*>(smem_raw);
-  unsigned char* cfb = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
-  cfb = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(cfb) + 127) & ~(size_t)127);
-  float2* cfs[2] = {reinterpret_cast<float2*>(cfb), reinterpret_cast<float2*>(cfb + a.cfbuf)};
-  unsigned long long* full = reinterpret_cast<unsigned long long*>(cfb + 2 * (size_t)a.cfbuf);
-  unsigned long long* empty = full + 2;
+  unsigned char* ring = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
+  ring = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(ring) + 127) & ~(size_t)127);
+  const int SB = a.stage_bytes, NST = a.nstages;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
+  unsigned long long* empty = full + NST;
   __shared__ int s_abort;
-  const int nwarps = blockDim.x / 32;
+  const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int Wp = a.Wp;
   const int Wp2 = Wp * Wp;
-  const int trash = Pg * Pg + threadIdx.x;      // target of slots beyond Wp^2
-
   const int4 it = a.items[blockIdx.x];
 
   if (threadIdx.x == 0) {
     s_abort = 0;
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], nwarps);
-    mbar_init(&empty[1], nwarps);
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], ncw);
+    }
     mbar_fence_init();
   }
   for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
   __syncthreads();
 
-  const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
-  auto run_end = [&](int j) { return max(j + 1, min(a.runend[j], it.z)); };
-  auto issue = [&](int start, int buf) {
-    const int c = a.rec[start].z;
-    mbar_expect_tx(&full[buf], cfcopy);
-    bulk_g2s(cfs[buf], a.cf.pad + (size_t)c * Wp2, cfcopy, &full[buf]);
-  };
-  if (threadIdx.x == 0) {
-    issue(it.y, 0);
-    const int e0 = run_end(it.y);
-    if (e0 < it.z) issue(e0, 1);
-  }
-
-  // RSTEP == 0: slot q of thread t owns residue k = q * blockDim + t.
-  // RSTEP > 0 (blockDim = RSTEP * Wp, MAXSLOTS * RSTEP = Wp): thread t owns
-  // the x residue t mod Wp and the y residues t / Wp + RSTEP * q, so the x
-  // part of the index arithmetic is done once per sample and the slots step
-  // down the rows.
-  int rx[RSTEP ? 1 : MAXSLOTS], rowoff[RSTEP ? 1 : MAXSLOTS];
-  bool live[RSTEP ? 1 : MAXSLOTS];
-  if (RSTEP) {
-    rx[0] = threadIdx.x % Wp;
-    rowoff[0] = threadIdx.x / Wp;
-    live[0] = true;
+  int nfill = 0;       // producer: stages filled
+  if (warp == ncw) {
+    if (!seg_produce<NPOL>(it, a.rec, a.svis, a.npol_total, a.pol0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full,
+                           empty, nfill)) {
+      if (lane == 0) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+      }
+    }
   } else {
+    // RSTEP == 0: slot q of thread t owns residue k = q * nthr + t.
+    // RSTEP > 0 (nthr = RSTEP * Wp, MAXSLOTS * RSTEP = Wp): thread t owns the
+    // x residue t mod Wp and the y residues t / Wp + RSTEP * q, so the x part
+    // of the index arithmetic is done once per sample and the slots step down
+    // the rows.
+    const int trash = Pg * Pg + threadIdx.x;     // target of slots beyond Wp^2
+    int rx[RSTEP ? 1 : MAXSLOTS], rowoff[RSTEP ? 1 : MAXSLOTS];
+    bool live[RSTEP ? 1 : MAXSLOTS];
+    if (RSTEP) {
+      rx[0] = threadIdx.x % Wp;
+      rowoff[0] = threadIdx.x / Wp;
+      live[0] = true;
+    } else {
 #pragma unroll
-    for (int q = 0; q < (RSTEP ? 1 : MAXSLOTS); ++q) {
-      const int k = q * blockDim.x + threadIdx.x;
-      live[q] = k < Wp2;
-      rx[q] = live[q] ? k % Wp : 0;
-      rowoff[q] = live[q] ? k / Wp : 0;   // ry
-    }
-  }
-  const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
-
-  unsigned fphase[2] = {0u, 0u}, ephase[2] = {0u, 0u};
-  bool ok = true;
-  int b = 0;
-  for (int j = it.y; j < it.z;) {
-    const int e = run_end(j);
-    if (!mbar_wait(&full[b], fphase[b])) {
-      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
-      ok = false;
-      break;
-    }
-    fphase[b] ^= 1u;
-    const float2* __restrict__ cf_s = cfs[b];
-    int4 r = a.rec[j];
-    float2 vv[NPOL];
-#pragma unroll
-    for (int p = 0; p < NPOL; ++p) vv[p] = a.svis[(size_t)j * a.npol_total + a.pol0 + p];
-    for (int i = j; i < e; ++i) {
-      // prefetch the next sample's record while this one is gridded
-      int4 rn = r;
-      float2 vn[NPOL];
-      if (i + 1 < e) {
-        rn = a.rec[i + 1];
-#pragma unroll
-        for (int p = 0; p < NPOL; ++p) vn[p] = a.svis[(size_t)(i + 1) * a.npol_total + a.pol0 + p];
+      for (int q = 0; q < (RSTEP ? 1 : MAXSLOTS); ++q) {
+        const int k = q * nthr + threadIdx.x;
+        live[q] = k < Wp2;
+        rx[q] = live[q] ? k % Wp : 0;
+        rowoff[q] = live[q] ? k / Wp : 0;   // ry
       }
-      const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
-      const int cb = px0 + Pg * py0;
-      const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
-      if (RSTEP) {
-        int jx = rx[0] - mx;
-        jx += (jx < 0) ? Wp : 0;
-        int jy0 = rowoff[0] - my;
-        jy0 += (jy0 < 0) ? Wp : 0;
-        int cell = cb + jx + Pg * jy0;
-        int tap = jx + Wp * jy0;
-        const int lim = Wp - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
+    }
+    const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
+    for (int nseg_done = 0;; ++nseg_done) {
+      const int stage = nseg_done % NST;
+      if (!mbar_wait(&full[stage], (unsigned)(nseg_done / NST) & 1u)) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+        break;
+      }
+      const unsigned char* sp = ring + (size_t)stage * SB;
+      const int cnt = *reinterpret_cast<const volatile int*>(sp + SB - 16);
+      if (cnt < 0) break;
+      const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
+      const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
+      const float2* vs = reinterpret_cast<const float2*>(sp + a.cfbuf + kSeg * 16);
+      for (int l = 0; l < cnt; ++l) {
+        const int4 r = recs[l];
+        float2 vv[NPOL];
 #pragma unroll
-        for (int q = 0; q < MAXSLOTS; ++q) {
-          const bool wrap = RSTEP * q >= lim;
-          const int c2 = wrap ? cell - PgW : cell;
-          const int t2 = wrap ? tap - Wp2 : tap;
-          const float2 c = cf_s[t2];
+        for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
+        const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
+        const int cb = px0 + Pg * py0;
+        const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
+        if (RSTEP) {
+          int jx = rx[0] - mx;
+          jx += (jx < 0) ? Wp : 0;
+          int jy0 = rowoff[0] - my;
+          jy0 += (jy0 < 0) ? Wp : 0;
+          int cell = cb + jx + Pg * jy0;
+          int tap = jx + Wp * jy0;
+          const int lim = Wp - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
 #pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            float2 g = acc_s[p * PG2 + c2];
-            g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
-            g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
-            acc_s[p * PG2 + c2] = g;
+          for (int q = 0; q < MAXSLOTS; ++q) {
+            const bool wrap = RSTEP * q >= lim;
+            const int c2 = wrap ? cell - PgW : cell;
+            const int t2 = wrap ? tap - Wp2 : tap;
+            const float2 c = cf_s[t2];
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+              float2 g = acc_s[p * PG2 + c2];
+              g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
+              g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
+              acc_s[p * PG2 + c2] = g;
+            }
+            cell += PgR;
+            tap += WpR;
           }
-          cell += PgR;
-          tap += WpR;
-        }
-      } else {
-#pragma unroll
-      for (int q = 0; q < MAXSLOTS; ++q) {
-        int jx = rx[q] - mx;
-        jx += (jx < 0) ? Wp : 0;
-        int jy = rowoff[q] - my;
-        jy += (jy < 0) ? Wp : 0;
-        const int cell = live[q] ? cb + jx + Pg * jy : trash;
-        const float2 c = cf_s[live[q] ? jx + Wp * jy : 0];
-#pragma unroll
-        for (int p = 0; p < NPOL; ++p) {
-          float2 g = acc_s[p * PG2 + cell];
-          g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
-          g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
-          acc_s[p * PG2 + cell] = g;
-        }
-      }
-      }
-      r = rn;
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) vv[p] = vn[p];
-    }
-    // this warp is done with buffer b
-    __syncwarp();
-    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
-    // producer: refill buffer b with the run after the next one
-    if (threadIdx.x == 0 && e < it.z) {
-      const int e2 = run_end(e);
-      if (e2 < it.z) {
-        if (!mbar_wait(&empty[b], ephase[b])) {
-          raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
-          s_abort = 1;
         } else {
-          fence_proxy_async_smem();
-          issue(e2, b);
+#pragma unroll
+          for (int q = 0; q < MAXSLOTS; ++q) {
+            int jx = rx[q] - mx;
+            jx += (jx < 0) ? Wp : 0;
+            int jy = rowoff[q] - my;
+            jy += (jy < 0) ? Wp : 0;
+            const int cell = live[q] ? cb + jx + Pg * jy : trash;
+            const float2 c = cf_s[live[q] ? jx + Wp * jy : 0];
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+              float2 g = acc_s[p * PG2 + cell];
+              g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
+              g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
+              acc_s[p * PG2 + cell] = g;
+            }
+          }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[stage]);
     }
-    ephase[b] ^= 1u;
-    j = e;
-    b ^= 1;
-    if (s_abort) {
-      ok = false;
-      break;
-    }
-  }
-  if (!ok) {
-    // let any copy still in flight land before the CTA's shared memory goes away
-    if (threadIdx.x == 0) {
-      mbar_wait(&full[0], fphase[0]);
-      mbar_wait(&full[1], fphase[1]);
-    }
-    s_abort = 1;
   }
   __syncthreads();
-  if (s_abort) return;
+  if (s_abort) {
+    if (warp == ncw && lane == 0) seg_drain(nfill, NST, full);
+    return;
+  }
   const int P = a.P, P2 = P * P;
   float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
   for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
@@ -815,17 +887,17 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
 }
 
 // Degridding of one work item on the padded layout: the grid tile (stride Pg,
-// zero outside the grid) is staged in shared memory, and the CF plane of each
-// run of equal-CF samples is brought in by a TMA bulk copy two runs ahead
-// (full/empty mbarriers, producer thread 0).  One warp per sample walks the
-// Wp x Wp taps 32 at a time: a half-warp reads 16 consecutive taps of one row,
-// so CF and grid reads fall on distinct banks; padded taps are exact zeros.
-// Four partial sums per lane hide the FMA latency; a warp shuffle combines
-// them (GridKernel.cc:99-137).
+// zero outside the grid) is staged in shared memory; the producer warp stages
+// segments (CF plane by TMA, records) into an NST-deep ring, and tap warp w
+// degrids the item's samples whose index in the item is w mod the number of
+// tap warps, so the warps work on different segments at once.  A warp walks a
+// sample's Wp x Wp taps 32 at a time: a half-warp reads 16 consecutive taps of
+// one row, so CF and grid reads fall on distinct banks; padded taps are exact
+// zeros.  Four partial sums per lane hide the FMA latency; a warp shuffle
+// combines them (GridKernel.cc:99-137).
 struct DegridTArgs {
   const int4* items;
   const int4* rec;
-  const int* runend;
   VisArgs v;
   CFView cf;
   const float2* grid;
@@ -833,25 +905,26 @@ struct DegridTArgs {
   int tile, ntx;
   long long ntiles;
   int smax, Pg, Wp, cfbuf;
+  int stage_bytes, nstages;
   float2* out;
   DevError* err;
 };
 
 template <int NPOL>
-__global__ void __launch_bounds__(kDegridThreads) k_degrid_t(DegridTArgs a) {
+__global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int Pg = a.Pg, PG2 = Pg * Pg;
   const int Wp = a.Wp, Wp2 = Wp * Wp;
   float2* g_s = reinterpret_cast<float2*>(smem_raw);
-  unsigned char* cfb = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
-  cfb = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(cfb) + 127) & ~(size_t)127);
-  float2* cfs[2] = {reinterpret_cast<float2*>(cfb), reinterpret_cast<float2*>(cfb + a.cfbuf)};
-  unsigned long long* full = reinterpret_cast<unsigned long long*>(cfb + 2 * (size_t)a.cfbuf);
-  unsigned long long* empty = full + 2;
+  unsigned char* ring = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
+  ring = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(ring) + 127) & ~(size_t)127);
+  const int SB = a.stage_bytes, NST = a.nstages;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
+  unsigned long long* empty = full + NST;
   __shared__ int s_abort;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
+  const int ncw = (blockDim.x >> 5) - 1;
 
   const int4 it = a.items[blockIdx.x];
   const long long gc = (long long)it.x / a.ntiles;
@@ -864,24 +937,11 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid_t(DegridTArgs a) {
 
   if (threadIdx.x == 0) {
     s_abort = 0;
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], nwarps);
-    mbar_init(&empty[1], nwarps);
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], ncw);
+    }
     mbar_fence_init();
-  }
-  const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
-  auto run_end = [&](int j) { return max(j + 1, min(a.runend[j], it.z)); };
-  auto issue = [&](int start, int buf) {
-    const int c = a.rec[start].z;
-    mbar_expect_tx(&full[buf], cfcopy);
-    bulk_g2s(cfs[buf], a.cf.pad + (size_t)c * Wp2, cfcopy, &full[buf]);
-  };
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    issue(it.y, 0);
-    const int e0 = run_end(it.y);
-    if (e0 < it.z) issue(e0, 1);
   }
   for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) {
     const int p = i / PG2, c = i % PG2;
@@ -892,113 +952,120 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid_t(DegridTArgs a) {
   }
   __syncthreads();
 
-  // lane's first tap and its grid-cell offset inside the footprint
-  const int jx0 = lane % Wp, jy0 = lane / Wp;
-  const int steps = Wp2 / 32;        // Wp is a multiple of 16: Wp^2 / 32 is a multiple of 8
-  const int rows_per_step = 32 / Wp; // 2 when Wp == 16, else 0 (wrap handled below)
-  unsigned fphase[2] = {0u, 0u}, ephase[2] = {0u, 0u};
-  bool ok = true;
-  int b = 0;
-  for (int j = it.y; j < it.z;) {
-    const int e = run_end(j);
-    if (!mbar_wait(&full[b], fphase[b])) {
-      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
-      ok = false;
-      break;
-    }
-    fphase[b] ^= 1u;
-    const float2* __restrict__ cf_s = cfs[b];
-    for (int i = j + warp; i < e; i += nwarps) {
-      const int4 r = a.rec[i];
-      const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
-      const int origin = px0 + Pg * py0;
-      float re[4][NPOL], im[4][NPOL];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int p = 0; p < NPOL; ++p) re[u][p] = im[u][p] = 0.f;
-      int tap = lane;
-      int jx = jx0;
-      int cell = origin + jx0 + Pg * jy0;
-      for (int st = 0; st < steps; st += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const float2 cv = cf_s[tap];
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            const float2 g = g_s[p * PG2 + cell];
-            re[u][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[u][p]));
-            im[u][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[u][p]));
-          }
-          tap += 32;
-          if (rows_per_step) {
-            cell += rows_per_step * Pg;
-          } else {
-            jx += 32;
-            const bool wrap = jx >= Wp;
-            jx = wrap ? jx - Wp : jx;
-            cell += wrap ? 32 - Wp + Pg : 32;
-          }
-        }
-      }
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
-        float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          sr += __shfl_xor_sync(0xffffffffu, sr, off);
-          si += __shfl_xor_sync(0xffffffffu, si, off);
-        }
-        re[0][p] = sr;
-        im[0][p] = si;
-      }
+  int nfill = 0;
+  if (warp == ncw) {
+    if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill)) {
       if (lane == 0) {
-        const long long s = r.w;
-        const long long row = s % a.v.nrow;
-        const int chan = (int)(s / a.v.nrow);
-        float pr, pi;
-        phasor_of(a.v, row, chan, &pr, &pi);
-        const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+      }
+    }
+  } else {
+    // lane's first tap and its grid-cell offset inside the footprint
+    const int jx0 = lane % Wp, jy0 = lane / Wp;
+    const int steps = Wp2 / 32;        // Wp is a multiple of 16: Wp^2 / 32 is a multiple of 8
+    const int rows_per_step = 32 / Wp; // 2 when Wp == 16, else 0 (wrap handled below)
+    for (int nseg = 0;; ++nseg) {
+      const int stage = nseg % NST;
+      if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+        break;
+      }
+      const unsigned char* sp = ring + (size_t)stage * SB;
+      const volatile int* hdr = reinterpret_cast<const volatile int*>(sp + SB - 16);
+      const int cnt = hdr[0];
+      if (cnt < 0) break;
+      const int g0 = hdr[1];
+      const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
+      const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
+      for (int l = (warp - g0 % ncw + ncw) % ncw; l < cnt; l += ncw) {
+        const int4 r = recs[l];
+        const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
+        const int origin = px0 + Pg * py0;
+        float re[4][NPOL], im[4][NPOL];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) re[u][p] = im[u][p] = 0.f;
+        int tap = lane;
+        int jx = jx0;
+        int cell = origin + jx0 + Pg * jy0;
+        for (int st = 0; st < steps; st += 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float2 cv = cf_s[tap];
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+              const float2 g = g_s[p * PG2 + cell];
+              re[u][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[u][p]));
+              im[u][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[u][p]));
+            }
+            tap += 32;
+            if (rows_per_step) {
+              cell += rows_per_step * Pg;
+            } else {
+              jx += 32;
+              const bool wrap = jx >= Wp;
+              jx = wrap ? jx - Wp : jx;
+              cell += wrap ? 32 - Wp + Pg : 32;
+            }
+          }
+        }
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) {
-          float cr = re[0][p], ci = im[0][p];
-          if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
-          a.out[(size_t)s * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
-                                                    __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
+          float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
+          float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, off);
+            si += __shfl_xor_sync(0xffffffffu, si, off);
+          }
+          re[0][p] = sr;
+          im[0][p] = si;
+        }
+        if (lane == 0) {
+          const long long s = r.w;
+          const long long row = s % a.v.nrow;
+          const int chan = (int)(s / a.v.nrow);
+          float pr, pi;
+          phasor_of(a.v, row, chan, &pr, &pi);
+          const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            float cr = re[0][p], ci = im[0][p];
+            if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
+            a.out[(size_t)s * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
+                                                      __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
+          }
         }
       }
-    }
-    __syncwarp();
-    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
-    if (threadIdx.x == 0 && e < it.z) {
-      const int e2 = run_end(e);
-      if (e2 < it.z) {
-        if (!mbar_wait(&empty[b], ephase[b])) {
-          raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
-          s_abort = 1;
-        } else {
-          fence_proxy_async_smem();
-          issue(e2, b);
-        }
-      }
-    }
-    ephase[b] ^= 1u;
-    j = e;
-    b ^= 1;
-    if (s_abort) {
-      ok = false;
-      break;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[stage]);
     }
   }
-  if (!ok && threadIdx.x == 0) {
-    mbar_wait(&full[0], fphase[0]);
-    mbar_wait(&full[1], fphase[1]);
-  }
+  __syncthreads();
+  if (s_abort && warp == ncw && lane == 0) seg_drain(nfill, NST, full);
 }
 
-size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf) {
-  return (size_t)npol * Pg * Pg * sizeof(float2) + 128 + 2 * (size_t)cfbuf + 4 * sizeof(unsigned long long);
+// shared memory of k_degrid_t: the grid tile per polarisation, then the ring
+static size_t degrid_t_tile_bytes(int npol, int Pg) { return (size_t)npol * Pg * Pg * sizeof(float2) + 128; }
+
+size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf, int nst) {
+  return degrid_t_tile_bytes(npol, Pg) + (size_t)nst * (seg_stage_bytes(cfbuf, 0) + 16);
+}
+
+// Ring depth of k_degrid_t: up to 12 stages (a few more than the tap warps,
+// which work on different segments), as many as fit with two CTAs per SM when
+// at least min_stages_two_ctas do, else as many as fit one CTA; 0 when not
+// even 2 fit.
+int degrid_t_stages(int npol, int Pg, int cfbuf) {
+  const size_t tile = degrid_t_tile_bytes(npol, Pg);
+  const size_t stage = (size_t)seg_stage_bytes(cfbuf, 0) + 16;
+  if (tile + min_stages_two_ctas(stage) * stage <= 113 * 1024)
+    return (int)std::min<size_t>(12, (113 * 1024 - tile) / stage);
+  if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(12, (227 * 1024 - tile) / stage);
+  return 0;
 }
 
 // prev[o] = o when sample (row, chan) with o = row * nchan + chan is on-grid,
@@ -1210,7 +1277,7 @@ template <int NPOL, int MAXSLOTS, int RSTEP>
 static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
   auto k = k_grid<NPOL, MAXSLOTS, RSTEP>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k<<<nitems, threads, smem, st>>>(g);
+  k<<<nitems, threads + 32, smem, st>>>(g);   // tap warps + the producer warp
   YG_COUNT_LAUNCH();
   return cudaGetLastError();
 }
@@ -1283,24 +1350,63 @@ static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, G
   return cudaErrorInvalidConfiguration;
 }
 
-// shared memory of k_grid: the guttered tile (Pg^2 + one trash cell per
-// thread) per polarisation, two padded CF buffers (Wp^2 taps) and 4 mbarriers
+// shared memory of k_grid: the guttered tile (Pg^2 + one trash cell per tap
+// thread) per polarisation, then the ring of segment stages and its 2 NST
+// mbarriers
 int grid_cf_buffer_bytes(int wpad) { return ((wpad * wpad * 8) + 127) / 128 * 128; }
 
 int grid_tile_stride(int tile, int wpad, int smax, bool varsup) { return tile + wpad - 1 + (varsup ? smax : 0); }
 
-size_t grid_smem_bytes(int npol, int Pg, int cfbuf) {
-  return (size_t)npol * ((size_t)Pg * Pg + 512) * sizeof(float2) + 128 + 2 * (size_t)cfbuf +
-         4 * sizeof(unsigned long long);
+static size_t grid_tile_bytes(int npol, int Pg, int nthr) {
+  return (size_t)npol * ((size_t)Pg * Pg + nthr) * sizeof(float2) + 128;
+}
+
+size_t grid_smem_bytes(int npol, int Pg, int cfbuf, int nthr, int nst) {
+  return grid_tile_bytes(npol, Pg, nthr) + (size_t)nst * (seg_stage_bytes(cfbuf, npol) + 16);
+}
+
+// Ring depth: up to 8 stages, as many as fit with two CTAs per SM when at
+// least min_stages_two_ctas do, else as many as fit one CTA; 0 when not even 2
+// fit.
+int grid_stages(int npol, int Pg, int cfbuf, int nthr) {
+  const size_t tile = grid_tile_bytes(npol, Pg, nthr);
+  const size_t stage = (size_t)seg_stage_bytes(cfbuf, npol) + 16;
+  if (tile + min_stages_two_ctas(stage) * stage <= 113 * 1024)
+    return (int)std::min<size_t>(8, (113 * 1024 - tile) / stage);
+  if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(8, (227 * 1024 - tile) / stage);
+  return 0;
+}
+
+// Tile side for a plan: the largest multiple of 8 (32..256) whose k_grid
+// tile leaves room for min_stages_two_ctas segment stages with two CTAs per
+// SM, else for 3 stages with one CTA per SM, for the polarisations of one pass.
+int grid_tile_for(int smax, int npol, bool varsup) {
+  const int wpad = ((2 * smax + 1) + 15) / 16 * 16;
+  const int cfbuf = grid_cf_buffer_bytes(wpad);
+  const GridShape sh = grid_shape(wpad);
+  if (sh.threads == 0) return 16;
+  const size_t budgets[2] = {113 * 1024, 227 * 1024};
+  for (int k = 0; k < 2; ++k) {
+    for (int npa : {npol, 2, 1}) {
+      if (npa > npol || npol % npa) continue;
+      const size_t stage = (size_t)seg_stage_bytes(cfbuf, npa) + 16;
+      const int nst = k == 0 ? min_stages_two_ctas(stage) : 3;
+      for (int t = 256; t >= 32; t -= 8) {
+        const int Pg = grid_tile_stride(t, wpad, smax, varsup);
+        if (grid_tile_bytes(npa, Pg, sh.threads) + nst * stage <= budgets[k]) return t;
+      }
+    }
+  }
+  return 16;
 }
 
 // Polarisations accumulated together in one k_grid pass: the most that fit
 // the shared-memory budget.
-int grid_pols_per_pass(int npol, int Pg, int cfbuf) {
+int grid_pols_per_pass(int npol, int Pg, int cfbuf, int nthr) {
   const int cands[3] = {4, 2, 1};
   for (int c : cands) {
     if (c > npol || npol % c) continue;
-    if (grid_smem_bytes(c, Pg, cfbuf) <= 227 * 1024) return c;
+    if (grid_stages(c, Pg, cfbuf, nthr) > 0) return c;
   }
   return 0;
 }
@@ -1343,9 +1449,11 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.scratch = scratch.as<float2>();
   g.npol_total = v.npol;
   g.err = err;
-  const int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf);
+  const int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
   if (npa == 0) return YG_ERR_UNSUPPORTED;
-  const size_t smem = grid_smem_bytes(npa, Pg, g.cfbuf);
+  g.nstages = grid_stages(npa, Pg, g.cfbuf, shape.threads);
+  g.stage_bytes = seg_stage_bytes(g.cfbuf, npa);
+  const size_t smem = grid_smem_bytes(npa, Pg, g.cfbuf, shape.threads, g.nstages);
   if (ev0) cudaEventRecord(ev0, st);
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
@@ -1394,7 +1502,6 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     DegridTArgs d;
     d.items = pl.items.as<int4>();
     d.rec = pl.rec.as<int4>();
-    d.runend = pl.runend.as<int>();
     d.v = v;
     d.cf = cf;
     d.grid = grid;
@@ -1410,18 +1517,21 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     d.cfbuf = grid_cf_buffer_bytes(cf.wpad);
     d.out = tmp_vals.as<float2>();
     d.err = err;
-    const size_t smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf);
-    if (smem <= 227 * 1024) {
+    d.nstages = degrid_t_stages(v.npol, d.Pg, d.cfbuf);
+    d.stage_bytes = seg_stage_bytes(d.cfbuf, 0);
+    const size_t smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
+    if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
+      const int threads = kDegridThreads + 32;   // tap warps + the producer warp
       if (v.npol == 1) {
         cudaFuncSetAttribute(k_degrid_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<1><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        k_degrid_t<1><<<pl.nitems, threads, smem, st>>>(d);
       } else if (v.npol == 2) {
         cudaFuncSetAttribute(k_degrid_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<2><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        k_degrid_t<2><<<pl.nitems, threads, smem, st>>>(d);
       } else {
         cudaFuncSetAttribute(k_degrid_t<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<4><<<pl.nitems, kDegridThreads, smem, st>>>(d);
+        k_degrid_t<4><<<pl.nitems, threads, smem, st>>>(d);
       }
       YG_COUNT_LAUNCH();
       if (ev1) cudaEventRecord(ev1, st);
