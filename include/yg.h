@@ -162,7 +162,9 @@ void yg_plan_destroy(yg_plan* plan);
 /* ---- tuning ---- */
 int yg_set_tile(yg_gridder* g, int32_t tile);      /* 0 = automatic */
 int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
-/* k_grid accumulation: 0 automatic, 1 in place in shared memory, 2 registers */
+/* k_grid thread layout: 0 or 1 the default, 2 and 3 halve / quarter the tap
+ * threads (each steps down twice / four times the rows); YG_ERR_UNSUPPORTED
+ * at the next grid call when the CF width has no such layout */
 int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */

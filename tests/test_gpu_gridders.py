@@ -262,3 +262,39 @@ def test_mfs_weights(ygmod, oracle_mod):
     og.initialise_grid(nx, nx, 1, 1, cell, cell)
     og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag))
     _check_grid(og, gg)
+
+
+# ---- wide CFs: the staged-CF ring (Wp 80) and taps from global memory (Wp 144) ----
+def _adopt_cf(og, gg):
+    """Gives the oracle the GPU's CF planes, so that the tap path is compared
+    on identical taps."""
+    gpu = gg.convolution_functions()
+    og.cache.cfs = [None if c is None else np.asfortranarray(c) for c in gpu]
+    og._flat = og.cache.flatten()
+
+
+@pytest.mark.parametrize("wmax", [6000.0, 12000.0])
+def test_wproject_wide_support(ygmod, oracle_mod, wmax):
+    """Supports of 35 and 67 cells.  The CF planes agree to 1e-5 of each
+    plane's peak; at these widths most taps are 1e-3 of the peak or less, so
+    the FFT's rounding (cuFFT against the oracle's FFT) reaches ~1e-4 of the
+    grid's L2 norm, and the tap path is compared on the GPU's own CFs."""
+    import oracle
+    ds = _data(duration=240.0, nchan=2, diameter=3000.0, seed=21)
+    nx, cell = 512, 40.0 * ARCSEC
+    params = {"wmax": wmax, "nwplanes": 5, "oversample": 4, "maxsupport": 1024, "cutoff": 1e-3}
+    og, gg = _run_pair("WProject", params, ds, nx, cell, 1)
+    assert gg.support()[0] == og.cache.support
+    assert og.cache.support >= 30
+    worst = 0.0
+    for a, b in zip(og.cache.cfs, gg.convolution_functions()):
+        worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+    assert worst < TOL, worst
+    end_to_end = rel_l2(np.stack(gg.grids()), np.stack(og.grids))
+    assert end_to_end < 1e-3, end_to_end
+    _adopt_cf(og, gg)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag))
+    _check_grid(og, gg)
+    model, _ = snapped_model(ds, nx, cell, max_nu=0.5, extra=8)
+    _check_degrid(og, gg, ds, model, cell)

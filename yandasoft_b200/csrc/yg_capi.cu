@@ -346,7 +346,7 @@ int yg_set_tile(yg_gridder* g, int32_t tile) {
 
 int yg_set_grid_variant(yg_gridder* g, int32_t variant) {
   return guarded([&] {
-    if (variant < 0 || variant > 2) throw yg::YgError{YG_ERR_ARG, "variant must be 0, 1 or 2"};
+    if (variant < 0 || variant > 3) throw yg::YgError{YG_ERR_ARG, "variant must be 0 to 3"};
     G(g).set_grid_mode(variant);
   });
 }

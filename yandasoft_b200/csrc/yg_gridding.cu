@@ -320,7 +320,7 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
                                             const float2* __restrict__ vis, int vis_stride, int vis_off,
                                             const float2* __restrict__ cfpad, int Wp2, int cfbuf, int SB, int NST,
                                             unsigned char* ring, unsigned long long* full,
-                                            unsigned long long* empty, int& seg) {
+                                            unsigned long long* empty, int& seg, bool stage_cf = true) {
   const int lane = threadIdx.x & 31;
   const unsigned fm = 0xffffffffu;
   const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
@@ -371,9 +371,13 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
       }
       __syncwarp();
       if (lane == 0) {
-        fence_proxy_async_smem();
-        mbar_expect_tx(&full[stage], cfcopy);
-        bulk_g2s(sp, cfpad + (size_t)cfi * Wp2, cfcopy, &full[stage]);
+        if (stage_cf) {
+          fence_proxy_async_smem();
+          mbar_expect_tx(&full[stage], cfcopy);
+          bulk_g2s(sp, cfpad + (size_t)cfi * Wp2, cfcopy, &full[stage]);
+        } else {
+          mbar_arrive(&full[stage]);
+        }
       }
       ++seg;
     }
@@ -412,7 +416,11 @@ __device__ __forceinline__ void seg_drain(int nfill, int NST, unsigned long long
 // and visibilities by the warp) into an NST-deep ring with full/empty
 // mbarriers, so the tap warps read nothing but shared memory and never wait
 // on a global load.
-template <int NPOL, int MAXSLOTS, int RSTEP>
+//
+// CFS false (CF planes too large for the ring): the stages carry records and
+// visibilities only and the taps are read from the padded CF cache in global
+// memory (L2).
+template <int NPOL, int MAXSLOTS, int RSTEP, bool CFS>
 __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nthr = blockDim.x - 32;              // tap threads
@@ -446,7 +454,7 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
   int nfill = 0;       // producer: stages filled
   if (warp == ncw) {
     if (!seg_produce<NPOL>(it, a.rec, a.svis, a.npol_total, a.pol0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full,
-                           empty, nfill)) {
+                           empty, nfill, CFS)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -485,11 +493,12 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
       const unsigned char* sp = ring + (size_t)stage * SB;
       const int cnt = *reinterpret_cast<const volatile int*>(sp + SB - 16);
       if (cnt < 0) break;
-      const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
+      const float2* __restrict__ cf_stage = reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
       const float2* vs = reinterpret_cast<const float2*>(sp + a.cfbuf + kSeg * 16);
       for (int l = 0; l < cnt; ++l) {
         const int4 r = recs[l];
+        const float2* __restrict__ cf_s = CFS ? cf_stage : a.cf.pad + (size_t)r.z * Wp2;
         float2 vv[NPOL];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
@@ -509,7 +518,7 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
             const bool wrap = RSTEP * q >= lim;
             const int c2 = wrap ? cell - PgW : cell;
             const int t2 = wrap ? tap - Wp2 : tap;
-            const float2 c = cf_s[t2];
+            const float2 c = CFS ? cf_s[t2] : __ldg(cf_s + t2);
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + c2];
@@ -528,7 +537,8 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
             int jy = rowoff[q] - my;
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
-            const float2 c = cf_s[live[q] ? jx + Wp * jy : 0];
+            const int tq = live[q] ? jx + Wp * jy : 0;
+            const float2 c = CFS ? cf_s[tq] : __ldg(cf_s + tq);
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + cell];
@@ -895,6 +905,31 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
 // one row, so CF and grid reads fall on distinct banks; padded taps are exact
 // zeros.  Four partial sums per lane hide the FMA latency; a warp shuffle
 // combines them (GridKernel.cc:99-137).
+// Sums V values over the warp with a transposing butterfly: each of the first
+// log2(V) exchange steps halves the values a lane carries, the remaining steps
+// add one value, so 2V - 1 + 5 - log2(V) shuffles replace 5V.  On return every
+// lane holds the warp total of value index lane >> (5 - log2 V).
+template <int V>
+__device__ __forceinline__ float warp_transpose_sum(float (&x)[V], int lane) {
+  static_assert(V == 2 || V == 4 || V == 8, "2, 4 or 8 values");
+  int off = 16;
+#pragma unroll
+  for (int h = V / 2; h >= 1; h /= 2) {
+    const bool up = (lane & off) != 0;
+#pragma unroll
+    for (int k = 0; k < h; ++k) {
+      const float send = up ? x[k] : x[k + h];
+      const float keep = up ? x[k + h] : x[k];
+      x[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+    off >>= 1;
+  }
+  float y = x[0];
+#pragma unroll
+  for (; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+  return y;
+}
+
 struct DegridTArgs {
   const int4* items;
   const int4* rec;
@@ -1012,32 +1047,32 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
             }
           }
         }
+        // values 2p (real) and 2p + 1 (imaginary) of polarisation p
+        float x[2 * NPOL];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) {
-          float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
-          float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) {
-            sr += __shfl_xor_sync(0xffffffffu, sr, off);
-            si += __shfl_xor_sync(0xffffffffu, si, off);
-          }
-          re[0][p] = sr;
-          im[0][p] = si;
+          x[2 * p] = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
+          x[2 * p + 1] = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
         }
-        if (lane == 0) {
+        constexpr int sh = NPOL == 4 ? 2 : (NPOL == 2 ? 3 : 4);   // 5 - log2(2 NPOL)
+        const float cr0 = warp_transpose_sum<2 * NPOL>(x, lane);
+        const float ci0 = __shfl_down_sync(0xffffffffu, cr0, 1 << sh);
+        const int v = lane >> sh;
+        if ((lane & ((1 << sh) - 1)) == 0 && (v & 1) == 0) {
+          const int p = v >> 1;
           const long long s = r.w;
           const long long row = s % a.v.nrow;
           const int chan = (int)(s / a.v.nrow);
           float pr, pi;
           phasor_of(a.v, row, chan, &pr, &pi);
-          const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            float cr = re[0][p], ci = im[0][p];
-            if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
-            a.out[(size_t)s * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
-                                                      __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
+          float cr = cr0, ci = ci0;
+          if (a.v.mfs) {
+            const float m = a.v.mfs[chan];
+            cr = __fmul_rn(cr, m);
+            ci = __fmul_rn(ci, m);
           }
+          a.out[(size_t)s * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
+                                                    __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
         }
       }
       __syncwarp();
@@ -1273,9 +1308,9 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
 }
 
 
-template <int NPOL, int MAXSLOTS, int RSTEP>
+template <int NPOL, int MAXSLOTS, int RSTEP, bool CFS = true>
 static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
-  auto k = k_grid<NPOL, MAXSLOTS, RSTEP>;
+  auto k = k_grid<NPOL, MAXSLOTS, RSTEP, CFS>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<nitems, threads + 32, smem, st>>>(g);   // tap warps + the producer warp
   YG_COUNT_LAUNCH();
@@ -1289,6 +1324,21 @@ struct GridShape {
   int threads, slots, rstep;
 };
 
+GridShape grid_shape(int Wp);
+
+// Row layouts with fewer tap threads and more slots per thread, selected by
+// the tuning variant: variant v > 1 divides the threads of the default row
+// layout by 2^(v-1) (each thread then steps down 2^(v-1) times as many rows).
+GridShape grid_shape_variant(int Wp, int variant) {
+  GridShape sh = grid_shape(Wp);
+  if (variant <= 1 || sh.rstep == 0) return sh;
+  for (int v = 1; v < variant; ++v) {
+    if (sh.rstep % 2 || sh.threads / 2 < 64 || (sh.threads / 2) % 32) return GridShape{0, 0, 0};
+    sh = GridShape{sh.threads / 2, sh.slots * 2, sh.rstep / 2};
+  }
+  return sh;
+}
+
 GridShape grid_shape(int Wp) {
   switch (Wp) {
     case 16: return GridShape{256, 1, 16};
@@ -1299,6 +1349,7 @@ GridShape grid_shape(int Wp) {
     case 96: return GridShape{384, 24, 4};
     case 112: return GridShape{448, 28, 4};
     case 128: return GridShape{512, 32, 4};
+    case 144: return GridShape{288, 72, 2};
     default: break;
   }
   const int W2 = Wp * Wp;
@@ -1318,12 +1369,34 @@ GridShape grid_shape(int Wp) {
   return best;
 }
 
+// CF taps from global memory: the row layouts of the widest CFs only
+template <int NPOL>
+static cudaError_t launch_grid_np_global(const GridKArgs& g, int nitems, size_t smem, GridShape sh,
+                                         cudaStream_t st) {
+  const int t = sh.threads;
+  switch (sh.slots * 1000 + sh.rstep) {
+    case 8008: return launch_grid_ms<NPOL, 8, 8, false>(g, nitems, t, smem, st);
+    case 20004: return launch_grid_ms<NPOL, 20, 4, false>(g, nitems, t, smem, st);
+    case 24004: return launch_grid_ms<NPOL, 24, 4, false>(g, nitems, t, smem, st);
+    case 28004: return launch_grid_ms<NPOL, 28, 4, false>(g, nitems, t, smem, st);
+    case 32004: return launch_grid_ms<NPOL, 32, 4, false>(g, nitems, t, smem, st);
+    case 72002: return launch_grid_ms<NPOL, 72, 2, false>(g, nitems, t, smem, st);
+    default: return cudaErrorInvalidConfiguration;
+  }
+}
+
 template <int NPOL>
 static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, GridShape sh, cudaStream_t st) {
   const int t = sh.threads;
   if (sh.rstep) {
     switch (sh.slots * 1000 + sh.rstep) {
       case 1016: return launch_grid_ms<NPOL, 1, 16>(g, nitems, t, smem, st);
+      case 2008: return launch_grid_ms<NPOL, 2, 8>(g, nitems, t, smem, st);
+      case 4004: return launch_grid_ms<NPOL, 4, 4>(g, nitems, t, smem, st);
+      case 8004: return launch_grid_ms<NPOL, 8, 4>(g, nitems, t, smem, st);
+      case 12004: return launch_grid_ms<NPOL, 12, 4>(g, nitems, t, smem, st);
+      case 16004: return launch_grid_ms<NPOL, 16, 4>(g, nitems, t, smem, st);
+      case 8002: return launch_grid_ms<NPOL, 8, 2>(g, nitems, t, smem, st);
       case 4008: return launch_grid_ms<NPOL, 4, 8>(g, nitems, t, smem, st);
       case 6008: return launch_grid_ms<NPOL, 6, 8>(g, nitems, t, smem, st);
       case 8008: return launch_grid_ms<NPOL, 8, 8>(g, nitems, t, smem, st);
@@ -1331,6 +1404,7 @@ static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, G
       case 24004: return launch_grid_ms<NPOL, 24, 4>(g, nitems, t, smem, st);
       case 28004: return launch_grid_ms<NPOL, 28, 4>(g, nitems, t, smem, st);
       case 32004: return launch_grid_ms<NPOL, 32, 4>(g, nitems, t, smem, st);
+      case 72002: return launch_grid_ms<NPOL, 72, 2>(g, nitems, t, smem, st);
       default: return cudaErrorInvalidConfiguration;
     }
   }
@@ -1397,7 +1471,13 @@ int grid_tile_for(int smax, int npol, bool varsup) {
       }
     }
   }
-  return 16;
+  // CF planes read from global memory: stages of records only, one CTA per SM
+  const size_t stage = (size_t)seg_stage_bytes(0, 1) + 16;
+  for (int t = 256; t >= 8; t -= 8) {
+    const int Pg = grid_tile_stride(t, wpad, smax, varsup);
+    if (grid_tile_bytes(1, Pg, sh.threads) + 4 * stage <= budgets[1]) return t;
+  }
+  return 8;
 }
 
 // Polarisations accumulated together in one k_grid pass: the most that fit
@@ -1415,12 +1495,11 @@ int grid_pols_per_pass(int npol, int Pg, int cfbuf, int nthr) {
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
               const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0,
               cudaEvent_t ev1, int mode) {
-  (void)mode;
   if (pl.nitems == 0) return YG_OK;
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
   const int P = pl.pad;
   const int Pg = grid_tile_stride(pl.tile, cf.wpad, pl.smax, cf.varsup != 0);
-  const GridShape shape = grid_shape(cf.wpad);
+  const GridShape shape = grid_shape_variant(cf.wpad, mode);
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
   const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
@@ -1449,8 +1528,15 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.scratch = scratch.as<float2>();
   g.npol_total = v.npol;
   g.err = err;
-  const int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
-  if (npa == 0) return YG_ERR_UNSUPPORTED;
+  // the last warp is the producer: the tap threads must fill whole warps
+  if (shape.threads % 32) return YG_ERR_UNSUPPORTED;
+  int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
+  const bool cf_global = npa == 0;      // CF planes too wide for the ring: taps from global memory
+  if (cf_global) {
+    g.cfbuf = 0;
+    npa = grid_pols_per_pass(v.npol, Pg, 0, shape.threads);
+    if (npa == 0) return YG_ERR_UNSUPPORTED;
+  }
   g.nstages = grid_stages(npa, Pg, g.cfbuf, shape.threads);
   g.stage_bytes = seg_stage_bytes(g.cfbuf, npa);
   const size_t smem = grid_smem_bytes(npa, Pg, g.cfbuf, shape.threads, g.nstages);
@@ -1458,12 +1544,16 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
     cudaError_t e;
-    switch (npa) {
-      case 1: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st); break;
-      case 2: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st); break;
-      case 4: e = launch_grid_np<4>(g, pl.nitems, smem, shape, st); break;
+    switch (npa * 2 + (cf_global ? 1 : 0)) {
+      case 2: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st); break;
+      case 4: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st); break;
+      case 8: e = launch_grid_np<4>(g, pl.nitems, smem, shape, st); break;
+      case 3: e = launch_grid_np_global<1>(g, pl.nitems, smem, shape, st); break;
+      case 5: e = launch_grid_np_global<2>(g, pl.nitems, smem, shape, st); break;
+      case 9: e = launch_grid_np_global<4>(g, pl.nitems, smem, shape, st); break;
       default: return YG_ERR_UNSUPPORTED;
     }
+    if (e == cudaErrorInvalidConfiguration) return YG_ERR_UNSUPPORTED;
     if (e != cudaSuccess) return YG_ERR_CUDA;
   }
   if (ev1) cudaEventRecord(ev1, st);
