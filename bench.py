@@ -397,6 +397,10 @@ def run_b200(args, w):
     smem_bytes = info["nvalid"] * taps * (16.0 * npol + 8.0)
     smem_peak = 148 * 128 * sm_hz
     smem_tbs = smem_bytes / (kgrid_ms / 1e3) / 1e12 if kgrid_ms > 0 else 0.0
+    # measured on a slice of config 1: 48.9 B read per sample (record + sorted
+    # visibilities), 0.84 of the padded-tile scratch written
+    pad = info["tile"] + 2 * support
+    traffic = int(48.9 * info["nvalid"] + 0.84 * info["nitems"] * npol * pad * pad * 8)
     line = {
         "metric": METRIC,
         "cf_form": "plain (tabulated CF)",
@@ -412,7 +416,9 @@ def run_b200(args, w):
                    "plan_build_s": round(t_plan, 3)},
         "roofline": {"bound": "hbm", "kernel": "k_grid", "achieved": round(achieved_gbs, 2),
                      "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved_gbs / hbm_peak, 4), "traffic": None,
+                     "frac": round(achieved_gbs / hbm_peak, 4), "traffic": traffic,
+                     "traffic_note": "DRAM bytes per k_grid launch, scaled by samples and items from an ncu "
+                                     "capture of a 2% slice (profiles/k_grid_k_degrid_t_config1_small.md)",
                      "kgrid_ms": round(kgrid_ms, 4), "kdegrid_ms": round(kdeg_ms, 4),
                      "binding": {"resource": "shared memory", "achieved": round(smem_tbs, 3),
                                  "peak": round(smem_peak / 1e12, 3), "unit": "TB/s",
