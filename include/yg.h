@@ -189,6 +189,47 @@ int yg_get_stream(yg_gridder* g, void** stream);
  * race on it and must be serialised by the caller. */
 int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk);
 
+/* ---- learned convolution function ----
+ * No counterpart in the reference.  A sinusoidal MLP (5 inputs: the tap's
+ * continuous uv offset, w, frequency, beam; 4 hidden layers of 64; real and
+ * imaginary part out; FP16 weights, FP32 accumulation) trained on the GPU on
+ * the gridder's own tabulated CFs (WProjectVisGridder::initConvolutionFunction,
+ * WProjectVisGridder.cc:435-726) and evaluated inside the grid and degrid
+ * kernels in place of the table.  WProject and WStackWProject only. */
+typedef struct {
+  int64_t ntrain;          /* training taps drawn from the tabulated CFs */
+  int32_t batch;           /* taps per Adam step */
+  int32_t steps;           /* Adam steps */
+  double lr;               /* peak learning rate (cosine decay to lr / 20) */
+  uint64_t seed;
+  int32_t nwplanes_train;  /* > the gridder's nwplanes: train on a denser table of this many
+                              planes over the same w range (built and released by the call) */
+  int32_t reserved;
+} yg_learn_params;
+
+typedef struct {
+  double final_loss;       /* mean squared tap error of the last minibatch, in units of the largest tap */
+  float train_ms;          /* GPU time of the Adam steps */
+  int32_t steps;
+  float scale;             /* the largest |tap| (network output unit) */
+  double cf_table_bytes;   /* device bytes of the tabulated CFs (packed + padded copies) */
+  double network_bytes;    /* bytes of the FP16 network */
+} yg_learn_report;
+
+int32_t yg_mlp_nparams(void);
+int yg_learned_train(yg_gridder* g, const yg_learn_params* p, yg_learn_report* rep);
+/* 0: tabulated CFs (default), 1: the learned network (YG_ERR_STATE before training) */
+int yg_set_cf_form(yg_gridder* g, int32_t form);
+int yg_learned_get_params(yg_gridder* g, float* params, float* scale);
+int yg_learned_set_params(yg_gridder* g, const float* params, float scale);
+/* the network's loss scale * sum |y - t|^2 over n taps and its gradient with
+ * respect to params (FP32 master weights; the forward pass uses them rounded
+ * to FP16), on host arrays: x is n x 5, t is n x 2, grad has yg_mlp_nparams() */
+int yg_mlp_loss_grad(const float* params, const float* x, const float* t, int64_t n, float scale, float* grad,
+                     double* loss);
+/* y (n x 2) of the network with params rounded to FP16, host arrays */
+int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y);
+
 #ifdef __cplusplus
 }
 #endif

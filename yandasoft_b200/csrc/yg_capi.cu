@@ -2,8 +2,10 @@
 // structures of include/yg.h and the C++ Gridder, and turns exceptions into
 // status codes plus a thread-local message (the reference's ASKAPCHECK /
 // AskapError convention, askap/gridding/*.cc).
+#include <algorithm>
 #include <cstring>
 #include <memory>
+#include <vector>
 #include <new>
 #include <string>
 
@@ -375,6 +377,101 @@ int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk) {
   return guarded([&] {
     yg::Chunk c = to_chunk(chunk);
     G(g).degrid_noalloc(c);
+  });
+}
+
+int32_t yg_mlp_nparams(void) { return yg::kMlpParams; }
+
+int yg_learned_train(yg_gridder* g, const yg_learn_params* p, yg_learn_report* rep) {
+  return guarded([&] {
+    if (!p) throw yg::YgError{YG_ERR_ARG, "learn parameters must not be NULL"};
+    yg::LearnParams lp;
+    lp.ntrain = p->ntrain;
+    lp.batch = p->batch;
+    lp.steps = p->steps;
+    lp.lr = p->lr;
+    lp.seed = p->seed;
+    if (lp.ntrain <= 0 || lp.batch <= 0 || lp.steps < 0 || !(lp.lr > 0.0))
+      throw yg::YgError{YG_ERR_ARG, "ntrain, batch and lr must be positive, steps non-negative"};
+    yg::LearnReport r;
+    G(g).learned_train(lp, p->nwplanes_train, &r);
+    if (rep) {
+      rep->final_loss = r.final_loss;
+      rep->train_ms = r.train_ms;
+      rep->steps = r.steps;
+      rep->scale = r.scale;
+      rep->cf_table_bytes = (double)G(g).cf_table_bytes();
+      rep->network_bytes = (double)yg::kMlpParams * 2.0;
+    }
+  });
+}
+
+int yg_set_cf_form(yg_gridder* g, int32_t form) {
+  return guarded([&] { G(g).set_cf_form(form); });
+}
+
+int yg_learned_get_params(yg_gridder* g, float* params, float* scale) {
+  return guarded([&] {
+    if (!params) throw yg::YgError{YG_ERR_ARG, "params must not be NULL"};
+    std::vector<float> p;
+    G(g).learned_params(p);
+    std::memcpy(params, p.data(), p.size() * sizeof(float));
+    if (scale) *scale = (float)G(g).learned_scale();
+  });
+}
+
+int yg_learned_set_params(yg_gridder* g, const float* params, float scale) {
+  return guarded([&] {
+    if (!params || !(scale > 0.f)) throw yg::YgError{YG_ERR_ARG, "params must be given and scale positive"};
+    G(g).set_learned_params(params, scale);
+  });
+}
+
+int yg_mlp_loss_grad(const float* params, const float* x, const float* t, int64_t n, float scale, float* grad,
+                     double* loss) {
+  return guarded([&] {
+    if (!params || !grad || n < 0 || (n > 0 && (!x || !t)))
+      throw yg::YgError{YG_ERR_ARG, "params, x, t and grad must be given"};
+    yg::DevBuf p, X, T, G_, L;
+    auto ck = [](cudaError_t e) {
+      if (e != cudaSuccess) throw yg::YgError{YG_ERR_CUDA, cudaGetErrorString(e)};
+    };
+    ck(p.ensure(yg::kMlpParamsPadded * sizeof(float)));
+    ck(X.ensure(std::max<int64_t>(1, n) * yg::kMlpIn * sizeof(float)));
+    ck(T.ensure(std::max<int64_t>(1, n) * 2 * sizeof(float)));
+    ck(G_.ensure(yg::kMlpParamsPadded * sizeof(float)));
+    ck(L.ensure(sizeof(double)));
+    ck(cudaMemcpy(p.p, params, yg::kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
+    if (n > 0) {
+      ck(cudaMemcpy(X.p, x, n * yg::kMlpIn * sizeof(float), cudaMemcpyHostToDevice));
+      ck(cudaMemcpy(T.p, t, n * 2 * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    const int rc = yg::mlp_grad(p.as<float>(), X.as<float>(), T.as<float>(), n, scale, G_.as<float>(),
+                                L.as<double>(), 0);
+    if (rc) throw yg::YgError{rc, "network gradient"};
+    ck(cudaMemcpy(grad, G_.p, yg::kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+    double l = 0.0;
+    ck(cudaMemcpy(&l, L.p, sizeof(double), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+  });
+}
+
+int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y) {
+  return guarded([&] {
+    if (!params || n < 0 || (n > 0 && (!x || !y))) throw yg::YgError{YG_ERR_ARG, "params, x and y must be given"};
+    yg::DevBuf p, w16, X, Y;
+    auto ck = [](cudaError_t e) {
+      if (e != cudaSuccess) throw yg::YgError{YG_ERR_CUDA, cudaGetErrorString(e)};
+    };
+    yg::LearnedNet net;
+    std::vector<float> v(params, params + yg::kMlpParams);
+    if (net.init(v, 0)) throw yg::YgError{YG_ERR_CUDA, "network set-up"};
+    ck(X.ensure(std::max<int64_t>(1, n) * yg::kMlpIn * sizeof(float)));
+    ck(Y.ensure(std::max<int64_t>(1, n) * 2 * sizeof(float)));
+    if (n > 0) ck(cudaMemcpy(X.p, x, n * yg::kMlpIn * sizeof(float), cudaMemcpyHostToDevice));
+    const int rc = yg::mlp_eval_batch(net.w16.as<__half>(), X.as<float>(), n, Y.as<float>(), 0);
+    if (rc) throw yg::YgError{rc, "network evaluation"};
+    if (n > 0) ck(cudaMemcpy(y, Y.p, n * 2 * sizeof(float), cudaMemcpyDeviceToHost));
   });
 }
 

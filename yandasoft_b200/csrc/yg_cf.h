@@ -66,10 +66,12 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
 // the sums of weights (one fused pass over the sorted samples).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
               const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st,
-              cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, int mode = 0);
+              cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, int mode = 0,
+              const struct LearnedCF* lcf = nullptr);
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
+                cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr,
+                const struct LearnedCF* lcf = nullptr);
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
 int grid_cf_buffer_bytes(int wpad);
 int grid_tile_for(int smax, int npol, bool varsup);

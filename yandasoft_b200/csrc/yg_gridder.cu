@@ -373,6 +373,13 @@ std::unique_ptr<Gridder> Gridder::clone() const {
   g->mfs_order_ = mfs_order_;
   g->tile_override_ = tile_override_;
   g->vmax_ = vmax_;
+  if (net_.ready) {
+    std::vector<float> p;
+    learned_params(p);
+    g->set_learned_params(p.data(), net_.scale);
+    g->learn_wnorm_ = learn_wnorm_;
+    g->cf_form_ = cf_form_;
+  }
   return g;
 }
 
@@ -863,8 +870,9 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
   const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
+  const LearnedCF lcf = learned_view();
   rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
-                     err_.as<DevError>(), stream_, k0, k1, grid_mode_),
+                     err_.as<DevError>(), stream_, k0, k1, grid_mode_, cf_form_ == 1 ? &lcf : nullptr),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
   cudaEventRecord(e1, stream_);
@@ -927,8 +935,9 @@ void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
   cudaEventCreate(&k0);
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
+  const LearnedCF lcf = learned_view();
   rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
-                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1),
+                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1, cf_form_ == 1 ? &lcf : nullptr),
            "degridding");
   cudaEventRecord(e1, stream_);
   check_error();
@@ -1113,4 +1122,114 @@ void Gridder::plan_samples(const Plan& pl, int* iu, int* iv, int* cfi, unsigned 
   cuda_check(cudaMemcpy(cfi, pl.cfi.p, n * 4, cudaMemcpyDeviceToHost), "cfi");
   cuda_check(cudaMemcpy(status, pl.status.p, n, cudaMemcpyDeviceToHost), "status");
 }
+}  // namespace yg
+
+namespace yg {
+
+// ---------------------------------------------------------------------------
+// learned convolution function
+// ---------------------------------------------------------------------------
+LearnedCF Gridder::learned_view() const {
+  LearnedCF L{};
+  if (!net_.ready || !wterm_d_.p) return L;
+  L.w16 = net_.w16.as<__half>();
+  L.wterm = wterm_d_.as<double>();
+  L.wnorm = learn_wnorm_;
+  L.scale = net_.scale;
+  L.os = os_;
+  return L;
+}
+
+size_t Gridder::cf_table_bytes() const {
+  return (size_t)cf_.total * sizeof(float2) + cf_.pad.bytes;
+}
+
+// Trains the network on this gridder's tabulated CFs, or (nw_train > its
+// plane count) on a denser table of nw_train planes spread linearly over the
+// same w range, built on the GPU for the purpose and released afterwards.
+void Gridder::learned_train(const LearnParams& lp, int nw_train, LearnReport* rep) {
+  throw_if(kind_ != Kind::WProject && kind_ != Kind::WStackWProject, YG_ERR_UNSUPPORTED,
+           "the learned CF covers the W-projection gridders (WProject, WStackWProject)");
+  throw_if(variablesupport_ || offsetsupport_, YG_ERR_UNSUPPORTED,
+           "the learned CF needs one common support without offsets");
+  build_cf();
+  if (!net_.ready) rc_check(net_.init(mlp_initial_params(lp.seed), stream_), "network set-up");
+  const int nw = ws_.nwplanes;
+  std::vector<double> wt(nw);
+  for (int i = 0; i < nw; ++i) wt[i] = wterm_cf(i);
+  double wn = 0.0;
+  for (double w : wt) wn = std::max(wn, std::fabs(w));
+  learn_wnorm_ = wn > 0.0 ? wn : 1.0;
+  cuda_check(wterm_d_.ensure(nw * sizeof(double)), "alloc");
+  cuda_check(cudaMemcpyAsync(wterm_d_.p, wt.data(), nw * sizeof(double), cudaMemcpyHostToDevice, stream_), "up");
+  if (nw_train > nw && nw_train > 1) {
+    CFCacheDev dense;
+    WProjCFParams p;
+    p.shape_x = nx_;
+    p.shape_y = ny_;
+    p.uvcell_u = uvcell_[0];
+    p.uvcell_v = uvcell_[1];
+    p.os = os_;
+    p.maxsupport = maxsupport_;
+    p.wterms.resize(nw_train);
+    const double w0 = wt.front(), w1 = wt.back();
+    for (int i = 0; i < nw_train; ++i) p.wterms[i] = w0 + (w1 - w0) * (double)i / (double)(nw_train - 1);
+    p.cutoff = cutoff_;
+    p.cutoff_abs = cutoff_abs_;
+    p.limitsupport = limitsupport_;
+    p.variablesupport = false;
+    p.offsetsupport = false;
+    p.alpha = alpha_;
+    rc_check(cf_build_wproject(dense, p, cfwork_, stream_), "dense CF table");
+    cfwork_.release();
+    throw_if(dense.support != cf_.support, YG_ERR_STATE, "dense CF table has another support");
+    DevBuf wd;
+    cuda_check(wd.ensure(nw_train * sizeof(double)), "alloc");
+    cuda_check(cudaMemcpyAsync(wd.p, p.wterms.data(), nw_train * sizeof(double), cudaMemcpyHostToDevice, stream_),
+               "up");
+    rc_check(net_.train(dense.view(), wd.as<double>(), learn_wnorm_, os_, lp, learn_X_, learn_T_, stream_, rep),
+             "training");
+    sync();
+  } else {
+    rc_check(net_.train(cf_.view(), wterm_d_.as<double>(), learn_wnorm_, os_, lp, learn_X_, learn_T_, stream_, rep),
+             "training");
+  }
+  learn_X_.release();
+  learn_T_.release();
+}
+
+void Gridder::set_cf_form(int form) {
+  throw_if(form != 0 && form != 1, YG_ERR_ARG, "CF form must be 0 (tabulated) or 1 (learned)");
+  throw_if(form == 1 && (!net_.ready || !wterm_d_.p), YG_ERR_STATE, "the learned CF has not been trained");
+  cf_form_ = form;
+}
+
+void Gridder::learned_params(std::vector<float>& out) const {
+  throw_if(!net_.ready, YG_ERR_STATE, "the learned CF has not been trained");
+  out.resize(kMlpParams);
+  cuda_check(cudaMemcpyAsync(out.data(), net_.p.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+             "download");
+  cuda_check(cudaStreamSynchronize(stream_), "sync");
+}
+
+void Gridder::set_learned_params(const float* p, float scale) {
+  ensure_device();
+  std::vector<float> v(p, p + kMlpParams);
+  rc_check(net_.init(v, stream_), "network set-up");
+  net_.scale = scale;
+  if (!wterm_d_.p && (kind_ == Kind::WProject || kind_ == Kind::WStackWProject)) {
+    const int nw = ws_.nwplanes;
+    std::vector<double> wt(nw);
+    double wn = 0.0;
+    for (int i = 0; i < nw; ++i) {
+      wt[i] = wterm_cf(i);
+      wn = std::max(wn, std::fabs(wt[i]));
+    }
+    learn_wnorm_ = wn > 0.0 ? wn : 1.0;
+    cuda_check(wterm_d_.ensure(nw * sizeof(double)), "alloc");
+    cuda_check(cudaMemcpyAsync(wterm_d_.p, wt.data(), nw * sizeof(double), cudaMemcpyHostToDevice, stream_), "up");
+  }
+  sync();
+}
+
 }  // namespace yg

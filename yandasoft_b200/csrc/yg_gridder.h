@@ -11,6 +11,8 @@
 #include "yg_cf.h"
 #include "yg_image.h"
 #include "yg_internal.h"
+#include "yg_learned.h"
+#include "yg_mlp.cuh"
 #include "yg_spheroidal.h"
 
 namespace yg {
@@ -123,6 +125,15 @@ class Gridder {
   }
   // degrid of a device-resident chunk with no device allocation (yg_noalloc.cu)
   void degrid_noalloc(Chunk& c);
+
+  // learned convolution function (no counterpart in the reference)
+  void learned_train(const LearnParams& lp, int nw_train, LearnReport* rep);
+  void set_cf_form(int form);                   // 0 tabulated, 1 learned
+  int cf_form() const { return cf_form_; }
+  void learned_params(std::vector<float>& out) const;
+  void set_learned_params(const float* p, float scale);
+  double learned_scale() const { return net_.scale; }
+  size_t cf_table_bytes() const;
   // per-sample on-grid position (with CF offset), CF index and status of a plan
   void plan_samples(const Plan& pl, int* iu, int* iv, int* cfi, unsigned char* status) const;
 
@@ -189,6 +200,11 @@ class Gridder {
 
   CFCacheDev cf_;
   bool cf_built_ = false;
+  LearnedNet net_;
+  int cf_form_ = 0;
+  DevBuf wterm_d_, learn_X_, learn_T_;
+  double learn_wnorm_ = 1.0;
+  LearnedCF learned_view() const;
   DevBuf grids_, sumw_, carry_, err_, chanmap_d_, rowok_d_, corr_d_;
   DevBuf up_uvw_, up_delay_, up_freq_, up_vis_, up_noise_, up_flag_, up_feed_;
   DevBuf scratch_, svis_, tmpvals_, cfwork_, img_tmp_, mfs_d_;

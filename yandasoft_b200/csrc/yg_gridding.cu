@@ -29,6 +29,7 @@
 #include <cstdio>
 
 #include "yg_internal.h"
+#include "yg_mlp.cuh"
 
 namespace yg {
 
@@ -237,6 +238,7 @@ struct GridKArgs {
   int npol_total;            // polarisations of the visibility cube
   int stage_bytes;           // bytes of one segment stage
   int nstages;               // depth of the segment ring
+  LearnedCF lcf;             // the network of the learned CF mode
   DevError* err;
 };
 
@@ -404,6 +406,26 @@ __device__ __forceinline__ void seg_drain(int nfill, int NST, unsigned long long
   }
 }
 
+// Named barrier over the tap warps (the producer warp does not take part).
+__device__ __forceinline__ void tap_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
+
+// Learned-CF mode: shared memory past the ring's barriers holds the network
+// (FP32 copies of the FP16 weights) and one evaluated CF plane.
+__host__ __device__ __forceinline__ size_t learned_smem_bytes(int Wp) {
+  return 16 + (size_t)kMlpParamsPadded * sizeof(float) + (size_t)Wp * Wp * sizeof(float2);
+}
+
+// The tap warps evaluate CF plane cfi (width w) into `plane` when the segment
+// changes CF, between two barriers of their own.
+__device__ __forceinline__ void learned_plane(const float* ws, const LearnedCF& L, int cfi, int w, int Wp,
+                                              float2* plane, int nthr, int& cur) {
+  if (cfi == cur) return;
+  tap_bar(nthr);
+  for (int q = threadIdx.x; q < Wp * Wp; q += nthr) plane[q] = mlp_tap(ws, L, cfi, q % Wp, q / Wp, w);
+  tap_bar(nthr);
+  cur = cfi;
+}
+
 // Gridding of one work item.  Thread/slot k of the tap warps owns the cells
 // with (x mod Wp, y mod Wp) = (k mod Wp, k / Wp): no two threads touch the
 // same cell, so every tap is accumulated in place in shared memory without
@@ -417,11 +439,14 @@ __device__ __forceinline__ void seg_drain(int nfill, int NST, unsigned long long
 // mbarriers, so the tap warps read nothing but shared memory and never wait
 // on a global load.
 //
-// CFS false (CF planes too large for the ring): the stages carry records and
-// visibilities only and the taps are read from the padded CF cache in global
-// memory (L2).
-template <int NPOL, int MAXSLOTS, int RSTEP, bool CFS>
-__global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
+// CFM selects where the taps come from: 0, the ring (CF plane by TMA); 1, the
+// padded CF cache in global memory through L2, for planes too large for the
+// ring (the stages then carry records and visibilities only); 2, the learned
+// CF: the tap warps evaluate the network for every tap of a new CF plane into
+// shared memory when a segment changes CF.
+template <int NPOL, int MAXSLOTS, int RSTEP, int CFM>
+__global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
+  constexpr bool CFS = CFM == 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nthr = blockDim.x - 32;              // tap threads
   const int ncw = nthr / 32;
@@ -433,12 +458,15 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
   const int SB = a.stage_bytes, NST = a.nstages;
   unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
   unsigned long long* empty = full + NST;
+  float* ws = reinterpret_cast<float*>((reinterpret_cast<size_t>(empty + NST) + 15) & ~(size_t)15);
+  float2* plane = reinterpret_cast<float2*>(ws + kMlpParamsPadded);
   __shared__ int s_abort;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int Wp = a.Wp;
   const int Wp2 = Wp * Wp;
   const int4 it = a.items[blockIdx.x];
+  if (CFM == 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
 
   if (threadIdx.x == 0) {
     s_abort = 0;
@@ -483,6 +511,7 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
       }
     }
     const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
+    int cur_cfi = -1;
     for (int nseg_done = 0;; ++nseg_done) {
       const int stage = nseg_done % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg_done / NST) & 1u)) {
@@ -496,9 +525,13 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
       const float2* __restrict__ cf_stage = reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
       const float2* vs = reinterpret_cast<const float2*>(sp + a.cfbuf + kSeg * 16);
+      if (CFM == 2) {
+        const int4 r0 = recs[0];
+        learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, nthr, cur_cfi);
+      }
       for (int l = 0; l < cnt; ++l) {
         const int4 r = recs[l];
-        const float2* __restrict__ cf_s = CFS ? cf_stage : a.cf.pad + (size_t)r.z * Wp2;
+        const float2* __restrict__ cf_s = CFM == 0 ? cf_stage : (CFM == 1 ? a.cf.pad + (size_t)r.z * Wp2 : plane);
         float2 vv[NPOL];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
@@ -518,7 +551,7 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
             const bool wrap = RSTEP * q >= lim;
             const int c2 = wrap ? cell - PgW : cell;
             const int t2 = wrap ? tap - Wp2 : tap;
-            const float2 c = CFS ? cf_s[t2] : __ldg(cf_s + t2);
+            const float2 c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + c2];
@@ -538,7 +571,7 @@ __global__ void __launch_bounds__(544) k_grid(GridKArgs a) {
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
             const int tq = live[q] ? jx + Wp * jy : 0;
-            const float2 c = CFS ? cf_s[tq] : __ldg(cf_s + tq);
+            const float2 c = CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + cell];
@@ -941,11 +974,15 @@ struct DegridTArgs {
   long long ntiles;
   int smax, Pg, Wp, cfbuf;
   int stage_bytes, nstages;
+  LearnedCF lcf;             // the network of the learned CF mode
   float2* out;
   DevError* err;
 };
 
-template <int NPOL>
+// CFM 0: CF planes by TMA into the ring; 2: the learned CF, evaluated by the
+// tap warps into shared memory when a segment changes CF (all tap warps then
+// share each segment's samples).
+template <int NPOL, int CFM>
 __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int Pg = a.Pg, PG2 = Pg * Pg;
@@ -956,10 +993,13 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   const int SB = a.stage_bytes, NST = a.nstages;
   unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
   unsigned long long* empty = full + NST;
+  float* ws = reinterpret_cast<float*>((reinterpret_cast<size_t>(empty + NST) + 15) & ~(size_t)15);
+  float2* plane = reinterpret_cast<float2*>(ws + kMlpParamsPadded);
   __shared__ int s_abort;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ncw = (blockDim.x >> 5) - 1;
+  if (CFM == 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
 
   const int4 it = a.items[blockIdx.x];
   const long long gc = (long long)it.x / a.ntiles;
@@ -989,7 +1029,8 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
 
   int nfill = 0;
   if (warp == ncw) {
-    if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill)) {
+    if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill,
+                        CFM == 0)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -1000,6 +1041,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
     const int jx0 = lane % Wp, jy0 = lane / Wp;
     const int steps = Wp2 / 32;        // Wp is a multiple of 16: Wp^2 / 32 is a multiple of 8
     const int rows_per_step = 32 / Wp; // 2 when Wp == 16, else 0 (wrap handled below)
+    int cur_cfi = -1;
     for (int nseg = 0;; ++nseg) {
       const int stage = nseg % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
@@ -1012,9 +1054,13 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
       const int cnt = hdr[0];
       if (cnt < 0) break;
       const int g0 = hdr[1];
-      const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
+      const float2* __restrict__ cf_s = CFM == 2 ? plane : reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
-      for (int l = (warp - g0 % ncw + ncw) % ncw; l < cnt; l += ncw) {
+      if (CFM == 2) {
+        const int4 r0 = recs[0];
+        learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, 32 * ncw, cur_cfi);
+      }
+      for (int l = CFM == 2 ? warp : (warp - g0 % ncw + ncw) % ncw; l < cnt; l += ncw) {
         const int4 r = recs[l];
         const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
         const int origin = px0 + Pg * py0;
@@ -1308,9 +1354,9 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
 }
 
 
-template <int NPOL, int MAXSLOTS, int RSTEP, bool CFS = true>
+template <int NPOL, int MAXSLOTS, int RSTEP, int CFM = 0>
 static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
-  auto k = k_grid<NPOL, MAXSLOTS, RSTEP, CFS>;
+  auto k = k_grid<NPOL, MAXSLOTS, RSTEP, CFM>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<nitems, threads + 32, smem, st>>>(g);   // tap warps + the producer warp
   YG_COUNT_LAUNCH();
@@ -1375,12 +1421,37 @@ static cudaError_t launch_grid_np_global(const GridKArgs& g, int nitems, size_t 
                                          cudaStream_t st) {
   const int t = sh.threads;
   switch (sh.slots * 1000 + sh.rstep) {
-    case 8008: return launch_grid_ms<NPOL, 8, 8, false>(g, nitems, t, smem, st);
-    case 20004: return launch_grid_ms<NPOL, 20, 4, false>(g, nitems, t, smem, st);
-    case 24004: return launch_grid_ms<NPOL, 24, 4, false>(g, nitems, t, smem, st);
-    case 28004: return launch_grid_ms<NPOL, 28, 4, false>(g, nitems, t, smem, st);
-    case 32004: return launch_grid_ms<NPOL, 32, 4, false>(g, nitems, t, smem, st);
-    case 72002: return launch_grid_ms<NPOL, 72, 2, false>(g, nitems, t, smem, st);
+    case 8008: return launch_grid_ms<NPOL, 8, 8, 1>(g, nitems, t, smem, st);
+    case 20004: return launch_grid_ms<NPOL, 20, 4, 1>(g, nitems, t, smem, st);
+    case 24004: return launch_grid_ms<NPOL, 24, 4, 1>(g, nitems, t, smem, st);
+    case 28004: return launch_grid_ms<NPOL, 28, 4, 1>(g, nitems, t, smem, st);
+    case 32004: return launch_grid_ms<NPOL, 32, 4, 1>(g, nitems, t, smem, st);
+    case 72002: return launch_grid_ms<NPOL, 72, 2, 1>(g, nitems, t, smem, st);
+    default: return cudaErrorInvalidConfiguration;
+  }
+}
+
+// learned CF: the row layouts of at most 256 tap threads (register budget of
+// the in-kernel network)
+GridShape grid_shape_learned(int Wp) {
+  switch (Wp) {
+    case 16: return GridShape{256, 1, 16};
+    case 32: return GridShape{256, 4, 8};
+    case 48: return GridShape{192, 12, 4};
+    case 64: return GridShape{256, 16, 4};
+    default: return GridShape{0, 0, 0};
+  }
+}
+
+template <int NPOL>
+static cudaError_t launch_grid_np_learned(const GridKArgs& g, int nitems, size_t smem, GridShape sh,
+                                          cudaStream_t st) {
+  const int t = sh.threads;
+  switch (sh.slots * 1000 + sh.rstep) {
+    case 1016: return launch_grid_ms<NPOL, 1, 16, 2>(g, nitems, t, smem, st);
+    case 4008: return launch_grid_ms<NPOL, 4, 8, 2>(g, nitems, t, smem, st);
+    case 12004: return launch_grid_ms<NPOL, 12, 4, 2>(g, nitems, t, smem, st);
+    case 16004: return launch_grid_ms<NPOL, 16, 4, 2>(g, nitems, t, smem, st);
     default: return cudaErrorInvalidConfiguration;
   }
 }
@@ -1494,12 +1565,13 @@ int grid_pols_per_pass(int npol, int Pg, int cfbuf, int nthr) {
 // Grids the samples of a plan onto `grid` (ngrid planes of (nx, ny, npol, nchan_img)).
 int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, int nx, int ny, int nchan_img,
               const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0,
-              cudaEvent_t ev1, int mode) {
+              cudaEvent_t ev1, int mode, const LearnedCF* lcf) {
+  const bool learned = lcf && lcf->w16;
   if (pl.nitems == 0) return YG_OK;
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
   const int P = pl.pad;
   const int Pg = grid_tile_stride(pl.tile, cf.wpad, pl.smax, cf.varsup != 0);
-  const GridShape shape = grid_shape_variant(cf.wpad, mode);
+  const GridShape shape = learned ? grid_shape_learned(cf.wpad) : grid_shape_variant(cf.wpad, mode);
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
   const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
@@ -1530,20 +1602,52 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.err = err;
   // the last warp is the producer: the tap threads must fill whole warps
   if (shape.threads % 32) return YG_ERR_UNSUPPORTED;
-  int npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
-  const bool cf_global = npa == 0;      // CF planes too wide for the ring: taps from global memory
-  if (cf_global) {
+  g.lcf = learned ? *lcf : LearnedCF{};
+  int npa;
+  bool cf_global = false;
+  size_t smem;
+  if (learned) {
+    // records-only stages, then the network and one evaluated CF plane
     g.cfbuf = 0;
-    npa = grid_pols_per_pass(v.npol, Pg, 0, shape.threads);
+    const size_t extra = learned_smem_bytes(cf.wpad);
+    npa = 0;
+    for (int c : {4, 2, 1}) {
+      if (c > v.npol || v.npol % c) continue;
+      const size_t st_c = (size_t)seg_stage_bytes(0, c) + 16;
+      if (grid_tile_bytes(c, Pg, shape.threads) + extra + 2 * st_c <= 227 * 1024) { npa = c; break; }
+    }
     if (npa == 0) return YG_ERR_UNSUPPORTED;
+    const size_t st_n = (size_t)seg_stage_bytes(0, npa) + 16;
+    const size_t tile_b = grid_tile_bytes(npa, Pg, shape.threads);
+    g.nstages = (int)std::min<size_t>(8, (227 * 1024 - tile_b - extra) / st_n);
+    g.stage_bytes = seg_stage_bytes(0, npa);
+    smem = grid_smem_bytes(npa, Pg, 0, shape.threads, g.nstages) + extra;
+  } else {
+    npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
+    cf_global = npa == 0;      // CF planes too wide for the ring: taps from global memory
+    if (cf_global) {
+      g.cfbuf = 0;
+      npa = grid_pols_per_pass(v.npol, Pg, 0, shape.threads);
+      if (npa == 0) return YG_ERR_UNSUPPORTED;
+    }
+    g.nstages = grid_stages(npa, Pg, g.cfbuf, shape.threads);
+    g.stage_bytes = seg_stage_bytes(g.cfbuf, npa);
+    smem = grid_smem_bytes(npa, Pg, g.cfbuf, shape.threads, g.nstages);
   }
-  g.nstages = grid_stages(npa, Pg, g.cfbuf, shape.threads);
-  g.stage_bytes = seg_stage_bytes(g.cfbuf, npa);
-  const size_t smem = grid_smem_bytes(npa, Pg, g.cfbuf, shape.threads, g.nstages);
   if (ev0) cudaEventRecord(ev0, st);
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
     cudaError_t e;
+    if (learned) {
+      switch (npa) {
+        case 1: e = launch_grid_np_learned<1>(g, pl.nitems, smem, shape, st); break;
+        case 2: e = launch_grid_np_learned<2>(g, pl.nitems, smem, shape, st); break;
+        default: e = launch_grid_np_learned<4>(g, pl.nitems, smem, shape, st); break;
+      }
+      if (e == cudaErrorInvalidConfiguration) return YG_ERR_UNSUPPORTED;
+      if (e != cudaSuccess) return YG_ERR_CUDA;
+      continue;
+    }
     switch (npa * 2 + (cf_global ? 1 : 0)) {
       case 2: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st); break;
       case 4: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st); break;
@@ -1583,11 +1687,14 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
 // Degrids the samples of a plan from `grid` and adds the result into vis.
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
+                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf) {
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
   bool done = false;
+  const bool learned = lcf && lcf->w16;
+  if (learned && (cf.wpad <= 0 || cf.wpad > 64 || !(v.npol == 1 || v.npol == 2 || v.npol == 4)))
+    return YG_ERR_UNSUPPORTED;
   if (pl.nitems > 0 && cf.pad && cf.wpad > 0 && cf.wpad <= 128 && (v.npol == 1 || v.npol == 2 || v.npol == 4)) {
     DegridTArgs d;
     d.items = pl.items.as<int4>();
@@ -1607,21 +1714,36 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     d.cfbuf = grid_cf_buffer_bytes(cf.wpad);
     d.out = tmp_vals.as<float2>();
     d.err = err;
-    d.nstages = degrid_t_stages(v.npol, d.Pg, d.cfbuf);
+    d.lcf = learned ? *lcf : LearnedCF{};
+    size_t smem;
+    if (learned) {
+      // records-only stages; the network and one evaluated plane after them
+      d.cfbuf = 0;
+      const size_t tile = degrid_t_tile_bytes(v.npol, d.Pg), extra = learned_smem_bytes(d.Wp);
+      const size_t stage = (size_t)seg_stage_bytes(0, 0) + 16;
+      d.nstages = tile + extra + 2 * stage <= 227 * 1024 ? (int)std::min<size_t>(8, (227 * 1024 - tile - extra) / stage)
+                                                          : 0;
+      if (d.nstages == 0) return YG_ERR_UNSUPPORTED;
+      smem = degrid_t_smem_bytes(v.npol, d.Pg, 0, d.nstages) + extra;
+    } else {
+      d.nstages = degrid_t_stages(v.npol, d.Pg, d.cfbuf);
+      smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
+    }
     d.stage_bytes = seg_stage_bytes(d.cfbuf, 0);
-    const size_t smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
     if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
       const int threads = kDegridThreads + 32;   // tap warps + the producer warp
-      if (v.npol == 1) {
-        cudaFuncSetAttribute(k_degrid_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<1><<<pl.nitems, threads, smem, st>>>(d);
-      } else if (v.npol == 2) {
-        cudaFuncSetAttribute(k_degrid_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<2><<<pl.nitems, threads, smem, st>>>(d);
-      } else {
-        cudaFuncSetAttribute(k_degrid_t<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_degrid_t<4><<<pl.nitems, threads, smem, st>>>(d);
+      auto launch = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<pl.nitems, threads, smem, st>>>(d);
+      };
+      switch (v.npol * 10 + (learned ? 2 : 0)) {
+        case 10: launch(k_degrid_t<1, 0>); break;
+        case 20: launch(k_degrid_t<2, 0>); break;
+        case 40: launch(k_degrid_t<4, 0>); break;
+        case 12: launch(k_degrid_t<1, 2>); break;
+        case 22: launch(k_degrid_t<2, 2>); break;
+        default: launch(k_degrid_t<4, 2>); break;
       }
       YG_COUNT_LAUNCH();
       if (ev1) cudaEventRecord(ev1, st);

@@ -36,7 +36,8 @@ EXPORTS = [
     "yg_get_sum_weights", "yg_get_grid", "yg_get_shape", "yg_get_stats", "yg_build_cf", "yg_plan_create",
     "yg_plan_grid", "yg_plan_degrid", "yg_plan_info", "yg_plan_samples", "yg_plan_destroy", "yg_set_tile", "yg_set_item_size",
     "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
-    "yg_set_grid_variant", "yg_degrid_noalloc",
+    "yg_set_grid_variant", "yg_degrid_noalloc", "yg_mlp_nparams", "yg_learned_train", "yg_set_cf_form",
+    "yg_learned_get_params", "yg_learned_set_params", "yg_mlp_loss_grad", "yg_mlp_eval",
 ]
 
 
@@ -51,6 +52,16 @@ class AskapError(RuntimeError):
 class yg_axes(ctypes.Structure):
     _fields_ = [("cell", D * 2), ("centre", D * 2), ("tangent", D * 2), ("has_freq", I32), ("reserved", I32),
                 ("freq_start", D), ("freq_end", D)]
+
+
+class yg_learn_params(ctypes.Structure):
+    _fields_ = [("ntrain", I64), ("batch", I32), ("steps", I32), ("lr", D), ("seed", ctypes.c_uint64),
+                ("nwplanes_train", I32), ("reserved", I32)]
+
+
+class yg_learn_report(ctypes.Structure):
+    _fields_ = [("final_loss", D), ("train_ms", ctypes.c_float), ("steps", I32), ("scale", ctypes.c_float),
+                ("cf_table_bytes", D), ("network_bytes", D)]
 
 
 class yg_chunk(ctypes.Structure):
@@ -106,6 +117,14 @@ def load(path: str | None = None):
     L.yg_get_kernel_times.argtypes = [P, P]
     L.yg_kernel_launch_count.restype = I64
     L.yg_kernel_launch_count.argtypes = []
+    L.yg_mlp_nparams.restype = I32
+    L.yg_mlp_nparams.argtypes = []
+    L.yg_learned_train.argtypes = [P, ctypes.POINTER(yg_learn_params), ctypes.POINTER(yg_learn_report)]
+    L.yg_set_cf_form.argtypes = [P, I32]
+    L.yg_learned_get_params.argtypes = [P, P, ctypes.POINTER(ctypes.c_float)]
+    L.yg_learned_set_params.argtypes = [P, P, ctypes.c_float]
+    L.yg_mlp_loss_grad.argtypes = [P, P, P, I64, ctypes.c_float, P, ctypes.POINTER(D)]
+    L.yg_mlp_eval.argtypes = [P, P, I64, P]
     _LIB = L
     return L
 
@@ -319,6 +338,29 @@ class IVisGridder:
         _check(self._lib.yg_is_model_empty(self.h, ctypes.byref(v)))
         return bool(v.value)
 
+    # ---- learned convolution function (no counterpart in the reference) ----
+    def learned_train(self, ntrain=1 << 22, batch=16384, steps=60000, lr=1e-2, seed=1, nwplanes_train=0):
+        """Trains the CF network on this gridder's tabulated CFs (or a denser
+        table of nwplanes_train planes); returns the training report."""
+        lp = yg_learn_params(int(ntrain), int(batch), int(steps), float(lr), int(seed), int(nwplanes_train), 0)
+        r = yg_learn_report()
+        _check(self._lib.yg_learned_train(self.h, ctypes.byref(lp), ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in yg_learn_report._fields_}
+
+    def set_cf_form(self, form):
+        """0: tabulated CFs, 1: the learned network."""
+        _check(self._lib.yg_set_cf_form(self.h, int(form)))
+
+    def learned_params(self):
+        p = np.zeros(mlp_nparams(), dtype=np.float32)
+        sc = ctypes.c_float()
+        _check(self._lib.yg_learned_get_params(self.h, p.ctypes.data, ctypes.byref(sc)))
+        return p, sc.value
+
+    def set_learned_params(self, params, scale):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        _check(self._lib.yg_learned_set_params(self.h, p.ctypes.data, float(scale)))
+
     # ---- plans (repeated passes over resident data) ----
     def plan(self, acc: Accessor) -> Plan:
         return Plan(self, acc)
@@ -413,6 +455,32 @@ class IVisGridder:
         keys = ["samples_gridded", "taps_gridded", "samples_degridded", "taps_degridded", "ms_grid", "ms_degrid",
                 "ms_cf", "cf_planes"]
         return dict(zip(keys, out.tolist()))
+
+
+def mlp_nparams() -> int:
+    return int(load().yg_mlp_nparams())
+
+
+def mlp_loss_grad(params, X, T, scale=1.0):
+    """(loss, gradient) of the learned-CF network on the GPU for taps X (n x 5)
+    with targets T (n x 2): loss = scale * sum |y - t|^2."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    g = np.zeros(mlp_nparams(), dtype=np.float32)
+    loss = D()
+    _check(load().yg_mlp_loss_grad(p.ctypes.data, X.ctypes.data, T.ctypes.data, X.shape[0], float(scale),
+                                   g.ctypes.data, ctypes.byref(loss)))
+    return loss.value, g
+
+
+def mlp_eval(params, X):
+    """Network outputs (n x 2) for inputs X (n x 5), weights rounded to FP16."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros((X.shape[0], 2), dtype=np.float32)
+    _check(load().yg_mlp_eval(p.ctypes.data, X.ctypes.data, X.shape[0], Y.ctypes.data))
+    return Y
 
 
 def kernel_launch_count() -> int:
