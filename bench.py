@@ -54,7 +54,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
     ap.add_argument("--tile", type=int, default=0, help="uv tile side (0 = automatic)")
-    ap.add_argument("--variant", type=int, default=0, help="k_grid accumulation variant (0 = automatic)")
+    ap.add_argument("--variant", type=int, default=0, help="k_grid thread layout variant (0 = automatic)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-CF leg")
+    ap.add_argument("--learned-rows", type=float, default=0.01, help="fraction of the track the learned leg times")
+    ap.add_argument("--learned-steps", type=int, default=60000, help="Adam steps of the learned CF")
     return ap.parse_args()
 
 
@@ -436,6 +439,11 @@ def run_b200(args, w):
     del plan, gg, gd, acc, acc_model, model_buf
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+    if not args.no_learned and w["gridder"] in ("WProject", "WStackWProject"):
+        try:
+            line["learned"] = learned_leg(args, w, d, ps, axes, img)
+        except Exception as e:  # the learned leg must not hide the plain result
+            line["learned"] = {"error": repr(e)}
     if not args.no_e2e:
         line["e2e"] = e2e_b200(args, w, d, ps, axes, img)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -449,6 +457,107 @@ def run_b200(args, w):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def learned_leg(args, w, d, ps, axes, img):
+    """The learned CF beside the tabulated one on the same data: the network is
+    trained on the GPU on a table of 257 w-planes (oversampling as configured),
+    then a degrid + grid step runs with the network evaluated inside the
+    kernels, on a contiguous slice of the track (the in-kernel network costs
+    far more per tap than a table lookup), in two forms: at the tabulated
+    offsets and planes (form 1) and at every sample's own offsets and w
+    (form 2, continuous).  Reports Mvis/s of the three forms on that slice,
+    CF memory, the degridded-visibility error of each learned form against
+    the tabulated one and of all three against the FP64 DFT of the model on a
+    sample of gridded visibilities, and the form kept: a learned form only
+    where its error against the tabulated path is at most 1e-3."""
+    import torch
+    from yandasoft_b200 import gridder as G
+    npol, nchan, nrow = d["npol"], d["nchan"], d["nrow"]
+    nr = max(1, int(nrow * args.learned_rows))
+    uvw = d["uvw"][:nr].contiguous()
+    vis = d["vis"][:, :, :nr].contiguous()
+    nvis = nr * nchan * npol
+    acc = G.Accessor(uvw, d["freq"], vis, shape=(nr, nchan, npol))
+    nx = w["nx"]
+    gl = G.VisGridderFactory.make(ps)
+    gl.initialiseGrid(axes, (nx, nx, npol, 1))
+    gl.build_cf()
+    support = gl.support()[0]
+    rep = gl.learned_train(steps=args.learned_steps, nwplanes_train=257, seed=w["seed"] + 11)
+    dense_bytes = 257 * w["oversample"] ** 2 * (2 * support + 1) ** 2 * 8
+    out = {"cf_form_kept": None, "trained_on": "257 w-planes x oversample %d (dense table built on the GPU)"
+                                                 % w["oversample"],
+           "train_steps": rep["steps"], "train_ms": round(rep["train_ms"], 1),
+           "final_loss": rep["final_loss"], "network_bytes": int(rep["network_bytes"]),
+           "cf_table_bytes": int(rep["cf_table_bytes"]), "cf_table_257_planes_bytes": int(dense_bytes),
+           "slice": "first %d of %d rows (%.2f%% of the track), all %d channels x %d pols"
+                    % (nr, nrow, 100.0 * nr / nrow, nchan, npol)}
+    results = {}
+    stream = None
+    for form in (0, 1, 2):
+        gg = gl.clone()
+        gg.set_cf_form(form)
+        gg.initialiseGrid(axes, (nx, nx, npol, 1))
+        gd = gl.clone()
+        gd.set_cf_form(form)
+        gd.initialiseDegrid(axes, img)
+        model_buf = torch.zeros_like(vis)
+        accm = G.Accessor(uvw, d["freq"], model_buf, shape=(nr, nchan, npol))
+        plan = gg.plan(acc)
+        stream = torch.cuda.ExternalStream(gg.stream_handle())
+        gd.degrid_plan(plan, accm)         # warm-up (and the model visibilities of this form)
+        gg.grid_plan(plan, acc)
+        gg.synchronize()
+        gd.synchronize()
+        vis_model = model_buf.clone()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gd.degrid_plan(plan, accm)
+        gg.grid_plan(plan, acc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        iu, iv, cfi, st = plan.samples(gg, acc)
+        results[form] = dict(ms=ms, vis=vis_model, status=st)
+        del plan, gg, gd, accm, model_buf
+    v0 = results[0]["vis"][0]
+    err_plain = {f: float(torch.linalg.norm(results[f]["vis"][0] - v0) / torch.linalg.norm(v0)) for f in (1, 2)}
+    # FP64 DFT of the model image at a sample of gridded (row, channel) points, pol 0
+    st = results[0]["status"]                     # (nr, nchan) Fortran
+    rows, chans = np.nonzero(st == 3)
+    rng = np.random.default_rng(5)
+    k = rng.choice(len(rows), min(4096, len(rows)), replace=False)
+    rows, chans = rows[k], chans[k]
+    cell = w["cell"] * ARCSEC
+    xs, ys = np.nonzero(img[:, :, 0, 0])
+    flux = torch.tensor(img[xs, ys, 0, 0].astype(np.float64), device="cuda")
+    lm = torch.tensor(np.stack([(xs - nx // 2) * cell, (ys - nx // 2) * cell], 1), device="cuda")
+    nn = torch.sqrt(1 - lm[:, 0] ** 2 - lm[:, 1] ** 2) - 1
+    U = d["uvw"][torch.tensor(rows, device="cuda")]
+    f = torch.tensor(d["freq_np"][chans], device="cuda")
+    ph = 2 * math.pi * (f / C_LIGHT)[:, None] * (U[:, 0:1] * lm[None, :, 0] + U[:, 1:2] * lm[None, :, 1]
+                                                 + U[:, 2:3] * nn[None, :])
+    dft = (flux[None] * torch.exp(1j * ph)).sum(1)
+    ri, ci = torch.tensor(rows, device="cuda"), torch.tensor(chans, device="cuda")
+    edft = {}
+    for f in (0, 1, 2):
+        pv = results[f]["vis"][0][ci, ri].to(torch.complex128)
+        edft[f] = float(torch.linalg.norm(pv - dft) / torch.linalg.norm(dft))
+    names = {0: "tabulated", 1: "learned_planes", 2: "learned_continuous"}
+    out.update({
+        "mvis_s": {names[f]: round(nvis / (results[f]["ms"] / 1e3) / 1e6, 3) for f in (0, 1, 2)},
+        "ms_per_step": {names[f]: round(results[f]["ms"], 3) for f in (0, 1, 2)},
+        "degrid_rel_err_vs_tabulated": {names[f]: err_plain[f] for f in (1, 2)},
+        "degrid_rel_err_vs_dft": {**{names[f]: edft[f] for f in (0, 1, 2)}, "samples": int(len(rows))},
+        "tolerance": 1e-3,
+    })
+    ok = [f for f in (1, 2) if err_plain[f] <= 1e-3]
+    out["cf_form_kept"] = (names[ok[0]] if ok else
+                           "tabulated (fallback: the learned forms differ from the tabulated path by more than 1e-3)")
+    return out
 
 
 def e2e_b200(args, w, d, ps, axes, img):

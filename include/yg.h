@@ -218,7 +218,10 @@ typedef struct {
 
 int32_t yg_mlp_nparams(void);
 int yg_learned_train(yg_gridder* g, const yg_learn_params* p, yg_learn_report* rep);
-/* 0: tabulated CFs (default), 1: the learned network (YG_ERR_STATE before training) */
+/* 0: tabulated CFs (default); 1: the learned network at the tabulated offsets
+ * and w planes; 2: the learned network at every sample's own fractional
+ * offsets and w (continuous, no oversampling or w-plane quantisation).
+ * YG_ERR_STATE before training. */
 int yg_set_cf_form(yg_gridder* g, int32_t form);
 int yg_learned_get_params(yg_gridder* g, float* params, float* scale);
 int yg_learned_set_params(yg_gridder* g, const float* params, float scale);

@@ -73,6 +73,9 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
                 cudaStream_t st, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr,
                 const struct LearnedCF* lcf = nullptr);
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st);
+// per sorted sample inputs of the continuous learned CF (once per plan)
+int plan_learned_inputs(Plan& pl, const double* uvw, const double* freq, double cellu, double cellv, int os,
+                        int nchan_img, const double* wstack, double wnorm, cudaStream_t st);
 int grid_cf_buffer_bytes(int wpad);
 int grid_tile_for(int smax, int npol, bool varsup);
 int grid_tile_stride(int tile, int wpad, int smax, bool varsup);

@@ -870,9 +870,9 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
   const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
-  const LearnedCF lcf = learned_view();
+  const LearnedCF lcf = learned_view_for(dc, const_cast<Plan&>(pl));
   rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
-                     err_.as<DevError>(), stream_, k0, k1, grid_mode_, cf_form_ == 1 ? &lcf : nullptr),
+                     err_.as<DevError>(), stream_, k0, k1, grid_mode_, cf_form_ != 0 ? &lcf : nullptr),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
   cudaEventRecord(e1, stream_);
@@ -935,9 +935,9 @@ void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
   cudaEventCreate(&k0);
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  const LearnedCF lcf = learned_view();
+  const LearnedCF lcf = learned_view_for(dc, pl);
   rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
-                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1, cf_form_ == 1 ? &lcf : nullptr),
+                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1, cf_form_ != 0 ? &lcf : nullptr),
            "degridding");
   cudaEventRecord(e1, stream_);
   check_error();
@@ -1140,6 +1140,29 @@ LearnedCF Gridder::learned_view() const {
   return L;
 }
 
+// The view for one grid or degrid call: the continuous form (2) also needs the
+// plan's per-sample inputs, made once per plan.
+LearnedCF Gridder::learned_view_for(const Chunk& dc, Plan& pl) {
+  LearnedCF L = learned_view();
+  if (cf_form_ != 2 || !L.w16) return L;
+  const double* wstack = nullptr;
+  if (kind_ == Kind::WStackWProject) {
+    if (!wstack_d_.p) {
+      std::vector<double> w(ws_stack_.nwplanes);
+      for (int g = 0; g < ws_stack_.nwplanes; ++g) w[g] = wterm_of(ws_stack_, g);
+      cuda_check(wstack_d_.ensure(w.size() * sizeof(double)), "alloc");
+      cuda_check(cudaMemcpyAsync(wstack_d_.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                 "up");
+    }
+    wstack = wstack_d_.as<double>();
+  }
+  rc_check(plan_learned_inputs(pl, dc.uvw, dc.freq, uvcell_[0], uvcell_[1], os_, nchan_, wstack, learn_wnorm_,
+                               stream_),
+           "continuous CF inputs");
+  L.ext = pl.ext.as<float4>();
+  return L;
+}
+
 size_t Gridder::cf_table_bytes() const {
   return (size_t)cf_.total * sizeof(float2) + cf_.pad.bytes;
 }
@@ -1199,8 +1222,9 @@ void Gridder::learned_train(const LearnParams& lp, int nw_train, LearnReport* re
 }
 
 void Gridder::set_cf_form(int form) {
-  throw_if(form != 0 && form != 1, YG_ERR_ARG, "CF form must be 0 (tabulated) or 1 (learned)");
-  throw_if(form == 1 && (!net_.ready || !wterm_d_.p), YG_ERR_STATE, "the learned CF has not been trained");
+  throw_if(form < 0 || form > 2, YG_ERR_ARG,
+           "CF form must be 0 (tabulated), 1 (learned, tabulated planes) or 2 (learned, continuous)");
+  throw_if(form != 0 && (!net_.ready || !wterm_d_.p), YG_ERR_STATE, "the learned CF has not been trained");
   cf_form_ = form;
 }
 

@@ -128,7 +128,7 @@ class Gridder {
 
   // learned convolution function (no counterpart in the reference)
   void learned_train(const LearnParams& lp, int nw_train, LearnReport* rep);
-  void set_cf_form(int form);                   // 0 tabulated, 1 learned
+  void set_cf_form(int form);  // 0 tabulated, 1 learned at the tabulated planes, 2 learned continuous
   int cf_form() const { return cf_form_; }
   void learned_params(std::vector<float>& out) const;
   void set_learned_params(const float* p, float scale);
@@ -202,9 +202,10 @@ class Gridder {
   bool cf_built_ = false;
   LearnedNet net_;
   int cf_form_ = 0;
-  DevBuf wterm_d_, learn_X_, learn_T_;
+  DevBuf wterm_d_, wstack_d_, learn_X_, learn_T_;
   double learn_wnorm_ = 1.0;
   LearnedCF learned_view() const;
+  LearnedCF learned_view_for(const Chunk& dc, Plan& pl);
   DevBuf grids_, sumw_, carry_, err_, chanmap_d_, rowok_d_, corr_d_;
   DevBuf up_uvw_, up_delay_, up_freq_, up_vis_, up_noise_, up_flag_, up_feed_;
   DevBuf scratch_, svis_, tmpvals_, cfwork_, img_tmp_, mfs_d_;

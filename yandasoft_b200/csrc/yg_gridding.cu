@@ -239,6 +239,7 @@ struct GridKArgs {
   int stage_bytes;           // bytes of one segment stage
   int nstages;               // depth of the segment ring
   LearnedCF lcf;             // the network of the learned CF mode
+  const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   DevError* err;
 };
 
@@ -322,15 +323,17 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
                                             const float2* __restrict__ vis, int vis_stride, int vis_off,
                                             const float2* __restrict__ cfpad, int Wp2, int cfbuf, int SB, int NST,
                                             unsigned char* ring, unsigned long long* full,
-                                            unsigned long long* empty, int& seg, bool stage_cf = true) {
+                                            unsigned long long* empty, int& seg, bool stage_cf = true,
+                                            const float4* __restrict__ ext = nullptr) {
   const int lane = threadIdx.x & 31;
   const unsigned fm = 0xffffffffu;
   const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
   seg = 0;
-  auto load = [&](int base, int4& r, float2 (&v)[NV > 0 ? NV : 1]) {
+  auto load = [&](int base, int4& r, float2 (&v)[NV > 0 ? NV : 1], float4& x) {
     const int i = base + lane;
     if (i < it.z) {
       r = rec[i];
+      if (ext) x = ext[i];
 #pragma unroll
       for (int p = 0; p < NV; ++p) v[p] = vis[(size_t)i * vis_stride + vis_off + p];
     } else {
@@ -344,11 +347,13 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
   };
   int4 r;
   float2 v[NV > 0 ? NV : 1];
-  load(it.y, r, v);
+  float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+  load(it.y, r, v, x);
   for (int base = it.y; base < it.z; base += 32) {
     int4 rn;
     float2 vn[NV > 0 ? NV : 1];
-    load(base + 32, rn, vn);                       // next window in flight
+    float4 xn = x;
+    load(base + 32, rn, vn, xn);                   // next window in flight
     const int nwin = min(32, it.z - base);
     const int zprev = __shfl_up_sync(fm, r.z, 1);
     unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || zprev != r.z));
@@ -364,6 +369,7 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
         float2* vs = reinterpret_cast<float2*>(sp + cfbuf + kSeg * 16);
 #pragma unroll
         for (int p = 0; p < NV; ++p) vs[(lane - h) * NV + p] = v[p];
+        if (ext) reinterpret_cast<float4*>(sp + cfbuf + kSeg * 16 + kSeg * NV * 8)[lane - h] = x;
       }
       const int cfi = __shfl_sync(fm, r.z, h);
       if (lane == 0) {
@@ -384,6 +390,7 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
       ++seg;
     }
     r = rn;
+    x = xn;
 #pragma unroll
     for (int p = 0; p < NV; ++p) v[p] = vn[p];
   }
@@ -426,6 +433,25 @@ __device__ __forceinline__ void learned_plane(const float* ws, const LearnedCF& 
   cur = cfi;
 }
 
+// Continuous learned CF: tap (jx, jy) of a sample with CF index cfi, width w,
+// at its own fractional offsets fracu/os + ru, fracv/os + rv and its own w
+// (network input xw), instead of the nearest tabulated offset and plane.
+__device__ __forceinline__ float2 mlp_tap_exact(const float* __restrict__ ws, const LearnedCF& L, int cfi, int jx,
+                                                int jy, int w, const float4& e) {
+  if (jx >= w || jy >= w) return make_float2(0.f, 0.f);
+  const int S = (w - 1) / 2;
+  const int fu = cfi % L.os, fv = (cfi / L.os) % L.os;
+  const float s1 = 1.f / (float)(S + 1);
+  float x[kMlpIn];
+  x[0] = ((float)(jx - S) + ((float)fu / (float)L.os + e.x)) * s1;
+  x[1] = ((float)(jy - S) + ((float)fv / (float)L.os + e.y)) * s1;
+  x[2] = e.z;
+  x[3] = 0.f;
+  x[4] = 0.f;
+  const float2 y = mlp_eval(ws, x);
+  return make_float2(y.x * L.scale, y.y * L.scale);
+}
+
 // Gridding of one work item.  Thread/slot k of the tap warps owns the cells
 // with (x mod Wp, y mod Wp) = (k mod Wp, k / Wp): no two threads touch the
 // same cell, so every tap is accumulated in place in shared memory without
@@ -443,9 +469,11 @@ __device__ __forceinline__ void learned_plane(const float* ws, const LearnedCF& 
 // padded CF cache in global memory through L2, for planes too large for the
 // ring (the stages then carry records and visibilities only); 2, the learned
 // CF: the tap warps evaluate the network for every tap of a new CF plane into
-// shared memory when a segment changes CF.
+// shared memory when a segment changes CF; 3, the continuous learned CF: every
+// tap thread evaluates the network for its own taps of every sample at the
+// sample's exact offsets and w (staged beside its record).
 template <int NPOL, int MAXSLOTS, int RSTEP, int CFM>
-__global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
+__global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
   constexpr bool CFS = CFM == 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nthr = blockDim.x - 32;              // tap threads
@@ -466,7 +494,7 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
   const int Wp = a.Wp;
   const int Wp2 = Wp * Wp;
   const int4 it = a.items[blockIdx.x];
-  if (CFM == 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
+  if (CFM >= 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
 
   if (threadIdx.x == 0) {
     s_abort = 0;
@@ -482,7 +510,7 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
   int nfill = 0;       // producer: stages filled
   if (warp == ncw) {
     if (!seg_produce<NPOL>(it, a.rec, a.svis, a.npol_total, a.pol0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full,
-                           empty, nfill, CFS)) {
+                           empty, nfill, CFS, CFM == 3 ? a.ext : nullptr)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -525,6 +553,7 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
       const float2* __restrict__ cf_stage = reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
       const float2* vs = reinterpret_cast<const float2*>(sp + a.cfbuf + kSeg * 16);
+      const float4* xs = reinterpret_cast<const float4*>(sp + a.cfbuf + kSeg * 16 + kSeg * NPOL * 8);
       if (CFM == 2) {
         const int4 r0 = recs[0];
         learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, nthr, cur_cfi);
@@ -532,6 +561,9 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
       for (int l = 0; l < cnt; ++l) {
         const int4 r = recs[l];
         const float2* __restrict__ cf_s = CFM == 0 ? cf_stage : (CFM == 1 ? a.cf.pad + (size_t)r.z * Wp2 : plane);
+        float4 xe = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (CFM == 3) xe = xs[l];
+        const int wcf = (r.y >> 20) & 0x7ff;
         float2 vv[NPOL];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
@@ -551,7 +583,8 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
             const bool wrap = RSTEP * q >= lim;
             const int c2 = wrap ? cell - PgW : cell;
             const int t2 = wrap ? tap - Wp2 : tap;
-            const float2 c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
+            const float2 c = CFM == 3 ? mlp_tap_exact(ws, a.lcf, r.z, t2 % Wp, t2 / Wp, wcf, xe)
+                                      : (CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2]);
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + c2];
@@ -571,7 +604,8 @@ __global__ void __launch_bounds__(CFM == 2 ? 288 : 544) k_grid(GridKArgs a) {
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
             const int tq = live[q] ? jx + Wp * jy : 0;
-            const float2 c = CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq];
+            const float2 c = CFM == 3 ? (live[q] ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe) : make_float2(0.f, 0.f))
+                                      : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + cell];
@@ -975,6 +1009,7 @@ struct DegridTArgs {
   int smax, Pg, Wp, cfbuf;
   int stage_bytes, nstages;
   LearnedCF lcf;             // the network of the learned CF mode
+  const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   float2* out;
   DevError* err;
 };
@@ -982,6 +1017,9 @@ struct DegridTArgs {
 // CFM 0: CF planes by TMA into the ring; 2: the learned CF, evaluated by the
 // tap warps into shared memory when a segment changes CF (all tap warps then
 // share each segment's samples).
+//
+// CFM 3: the continuous learned CF, every lane evaluating the network for its
+// taps of every sample at the sample's exact offsets and w.
 template <int NPOL, int CFM>
 __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -999,7 +1037,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ncw = (blockDim.x >> 5) - 1;
-  if (CFM == 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
+  if (CFM >= 2) mlp_load_smem(a.lcf.w16, ws, threadIdx.x, blockDim.x);
 
   const int4 it = a.items[blockIdx.x];
   const long long gc = (long long)it.x / a.ntiles;
@@ -1030,7 +1068,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   int nfill = 0;
   if (warp == ncw) {
     if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill,
-                        CFM == 0)) {
+                        CFM == 0, CFM == 3 ? a.ext : nullptr)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -1056,12 +1094,16 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
       const int g0 = hdr[1];
       const float2* __restrict__ cf_s = CFM == 2 ? plane : reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
+      const float4* xs = reinterpret_cast<const float4*>(sp + a.cfbuf + kSeg * 16);
       if (CFM == 2) {
         const int4 r0 = recs[0];
         learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, 32 * ncw, cur_cfi);
       }
       for (int l = CFM == 2 ? warp : (warp - g0 % ncw + ncw) % ncw; l < cnt; l += ncw) {
         const int4 r = recs[l];
+        float4 xe = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (CFM == 3) xe = xs[l];
+        const int wcf = (r.y >> 20) & 0x7ff;
         const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
         const int origin = px0 + Pg * py0;
         float re[4][NPOL], im[4][NPOL];
@@ -1075,7 +1117,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
         for (int st = 0; st < steps; st += 4) {
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const float2 cv = cf_s[tap];
+            const float2 cv = CFM == 3 ? mlp_tap_exact(ws, a.lcf, r.z, tap % Wp, tap / Wp, wcf, xe) : cf_s[tap];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               const float2 g = g_s[p * PG2 + cell];
@@ -1245,6 +1287,9 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   const long long n = a.nrow * (long long)a.nchan;
   pl.nsamples = n;
   pl.prev_ready = false;
+  pl.ext_ready = false;
+  pl.mbits = a.mbits;
+  pl.ncf = a.cf.ncf;
   pl.nrow = a.nrow;
   pl.nchan = a.nchan;
   pl.npol = a.npol;
@@ -1448,10 +1493,14 @@ static cudaError_t launch_grid_np_learned(const GridKArgs& g, int nitems, size_t
                                           cudaStream_t st) {
   const int t = sh.threads;
   switch (sh.slots * 1000 + sh.rstep) {
-    case 1016: return launch_grid_ms<NPOL, 1, 16, 2>(g, nitems, t, smem, st);
-    case 4008: return launch_grid_ms<NPOL, 4, 8, 2>(g, nitems, t, smem, st);
-    case 12004: return launch_grid_ms<NPOL, 12, 4, 2>(g, nitems, t, smem, st);
-    case 16004: return launch_grid_ms<NPOL, 16, 4, 2>(g, nitems, t, smem, st);
+    case 1016: return g.ext ? launch_grid_ms<NPOL, 1, 16, 3>(g, nitems, t, smem, st)
+                            : launch_grid_ms<NPOL, 1, 16, 2>(g, nitems, t, smem, st);
+    case 4008: return g.ext ? launch_grid_ms<NPOL, 4, 8, 3>(g, nitems, t, smem, st)
+                            : launch_grid_ms<NPOL, 4, 8, 2>(g, nitems, t, smem, st);
+    case 12004: return g.ext ? launch_grid_ms<NPOL, 12, 4, 3>(g, nitems, t, smem, st)
+                             : launch_grid_ms<NPOL, 12, 4, 2>(g, nitems, t, smem, st);
+    case 16004: return g.ext ? launch_grid_ms<NPOL, 16, 4, 3>(g, nitems, t, smem, st)
+                             : launch_grid_ms<NPOL, 16, 4, 2>(g, nitems, t, smem, st);
     default: return cudaErrorInvalidConfiguration;
   }
 }
@@ -1603,6 +1652,8 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   // the last warp is the producer: the tap threads must fill whole warps
   if (shape.threads % 32) return YG_ERR_UNSUPPORTED;
   g.lcf = learned ? *lcf : LearnedCF{};
+  g.ext = learned ? lcf->ext : nullptr;
+  const int xv = g.ext ? 2 : 0;          // the continuous inputs take two float2 slots per sample
   int npa;
   bool cf_global = false;
   size_t smem;
@@ -1613,15 +1664,15 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     npa = 0;
     for (int c : {4, 2, 1}) {
       if (c > v.npol || v.npol % c) continue;
-      const size_t st_c = (size_t)seg_stage_bytes(0, c) + 16;
+      const size_t st_c = (size_t)seg_stage_bytes(0, c + xv) + 16;
       if (grid_tile_bytes(c, Pg, shape.threads) + extra + 2 * st_c <= 227 * 1024) { npa = c; break; }
     }
     if (npa == 0) return YG_ERR_UNSUPPORTED;
-    const size_t st_n = (size_t)seg_stage_bytes(0, npa) + 16;
+    const size_t st_n = (size_t)seg_stage_bytes(0, npa + xv) + 16;
     const size_t tile_b = grid_tile_bytes(npa, Pg, shape.threads);
     g.nstages = (int)std::min<size_t>(8, (227 * 1024 - tile_b - extra) / st_n);
-    g.stage_bytes = seg_stage_bytes(0, npa);
-    smem = grid_smem_bytes(npa, Pg, 0, shape.threads, g.nstages) + extra;
+    g.stage_bytes = seg_stage_bytes(0, npa + xv);
+    smem = tile_b + (size_t)g.nstages * st_n + extra;
   } else {
     npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
     cf_global = npa == 0;      // CF planes too wide for the ring: taps from global memory
@@ -1715,21 +1766,24 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
     d.out = tmp_vals.as<float2>();
     d.err = err;
     d.lcf = learned ? *lcf : LearnedCF{};
+    d.ext = learned ? lcf->ext : nullptr;
+    const int xv = d.ext ? 2 : 0;
     size_t smem;
     if (learned) {
-      // records-only stages; the network and one evaluated plane after them
+      // records-only stages (plus the continuous inputs); the network and one
+      // evaluated plane after them
       d.cfbuf = 0;
       const size_t tile = degrid_t_tile_bytes(v.npol, d.Pg), extra = learned_smem_bytes(d.Wp);
-      const size_t stage = (size_t)seg_stage_bytes(0, 0) + 16;
+      const size_t stage = (size_t)seg_stage_bytes(0, xv) + 16;
       d.nstages = tile + extra + 2 * stage <= 227 * 1024 ? (int)std::min<size_t>(8, (227 * 1024 - tile - extra) / stage)
                                                           : 0;
       if (d.nstages == 0) return YG_ERR_UNSUPPORTED;
-      smem = degrid_t_smem_bytes(v.npol, d.Pg, 0, d.nstages) + extra;
+      smem = tile + (size_t)d.nstages * stage + extra;
     } else {
       d.nstages = degrid_t_stages(v.npol, d.Pg, d.cfbuf);
       smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
     }
-    d.stage_bytes = seg_stage_bytes(d.cfbuf, 0);
+    d.stage_bytes = seg_stage_bytes(d.cfbuf, xv);
     if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
       const int threads = kDegridThreads + 32;   // tap warps + the producer warp
@@ -1737,13 +1791,16 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<pl.nitems, threads, smem, st>>>(d);
       };
-      switch (v.npol * 10 + (learned ? 2 : 0)) {
+      switch (v.npol * 10 + (learned ? (d.ext ? 3 : 2) : 0)) {
         case 10: launch(k_degrid_t<1, 0>); break;
         case 20: launch(k_degrid_t<2, 0>); break;
         case 40: launch(k_degrid_t<4, 0>); break;
         case 12: launch(k_degrid_t<1, 2>); break;
         case 22: launch(k_degrid_t<2, 2>); break;
-        default: launch(k_degrid_t<4, 2>); break;
+        case 42: launch(k_degrid_t<4, 2>); break;
+        case 13: launch(k_degrid_t<1, 3>); break;
+        case 23: launch(k_degrid_t<2, 3>); break;
+        default: launch(k_degrid_t<4, 3>); break;
       }
       YG_COUNT_LAUNCH();
       if (ev1) cudaEventRecord(ev1, st);
@@ -1829,6 +1886,51 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
   k_update_carry<<<1, 32, 0, st>>>(prev + (n - 1), pl.nrow, pl.nchan, v.npol, tmp_vals.as<float2>(), 0, carry);
   YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaGetLastError());
+  return YG_OK;
+}
+
+// Continuous learned CF, once per plan: for every sorted sample the residue of
+// its fractional offsets beyond the tabulated fraction, ru = (t - nint(t)) / os
+// with t = os (iu - u f / (c cellu)) and likewise rv, and its own w (minus its
+// w-stack's w term) over wnorm.  Neither residue changes the indices: they
+// only feed the network.
+__global__ void k_learned_inputs(const int4* __restrict__ rec, const unsigned long long* __restrict__ key,
+                                 long long nvalid, const double* __restrict__ uvw, const double* __restrict__ freq,
+                                 long long nrow, double cellu, double cellv, int os, int mbits, int ncf,
+                                 long long ntiles, int nchan_img, const double* __restrict__ wstack, double wnorm,
+                                 float4* __restrict__ out) {
+  const double C = 299792458.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
+    const long long s = rec[i].w;
+    const long long row = s % nrow;
+    const int chan = (int)(s / nrow);
+    const double f = freq[chan];
+    const double us = uvw[3 * row] * f / (C * cellu);
+    const double vs = uvw[3 * row + 1] * f / (C * cellv);
+    const double tu = os * ((double)nint_d(us) - us);
+    const double tv = os * ((double)nint_d(vs) - vs);
+    double w = uvw[3 * row + 2] * f / C;
+    if (wstack) {
+      const long long gc = (long long)((key[i] >> mbits) / (unsigned long long)ncf) / ntiles;
+      w -= wstack[gc / nchan_img];
+    }
+    out[i] = make_float4((float)((tu - (double)nint_d(tu)) / os), (float)((tv - (double)nint_d(tv)) / os),
+                         (float)(w / wnorm), 0.f);
+  }
+}
+
+int plan_learned_inputs(Plan& pl, const double* uvw, const double* freq, double cellu, double cellv, int os,
+                        int nchan_img, const double* wstack, double wnorm, cudaStream_t st) {
+  if (pl.ext_ready) return YG_OK;
+  YG_CUDA_TRY(pl.ext.ensure((size_t)std::max(1ll, pl.nvalid) * sizeof(float4)));
+  if (pl.nvalid > 0) {
+    k_learned_inputs<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(
+        pl.rec.as<int4>(), pl.key.as<unsigned long long>(), pl.nvalid, uvw, freq, pl.nrow, cellu, cellv, os, pl.mbits,
+        pl.ncf, (long long)pl.ntx * pl.nty, nchan_img, wstack, wnorm, pl.ext.as<float4>());
+    YG_COUNT_LAUNCH();
+    YG_CUDA_TRY(cudaGetLastError());
+  }
+  pl.ext_ready = true;
   return YG_OK;
 }
 

@@ -108,6 +108,9 @@ struct Plan {
   DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
   DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
   DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
+  DevBuf ext;                   // continuous learned CF: per sorted sample (ru, rv, w, 0)
+  bool ext_ready = false;
+  int mbits = 0, ncf = 0;       // sort-key layout
   double taps = 0;              // sum of (2S+1)^2 over valid samples (per pol)
 };
 

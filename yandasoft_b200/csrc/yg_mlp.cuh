@@ -43,8 +43,9 @@ __device__ __forceinline__ void mlp_load_smem(const __half* __restrict__ w16, fl
 
 // One tap through the network, weights (FP32 copies of the FP16 values) in
 // shared memory.  Every lane of a warp reads the same weight at the same
-// time, so the loads are broadcasts.
-__device__ __forceinline__ float2 mlp_eval(const float* __restrict__ ws, const float (&x)[kMlpIn]) {
+// time, so the loads are broadcasts.  Kept out of line: its 13k multiply-adds
+// would otherwise be copied into every unrolled tap slot of the callers.
+static __device__ __noinline__ float2 mlp_eval(const float* __restrict__ ws, const float (&x)[kMlpIn]) {
   float h[kMlpH];
 #pragma unroll
   for (int j = 0; j < kMlpH; ++j) {
@@ -98,6 +99,7 @@ struct LearnedCF {
   double wnorm;             // w is divided by this
   float scale;              // tap = y * scale
   int os;
+  const float4* ext;        // continuous form: per sorted sample of the plan (ru, rv, w / wnorm, 0); null = planes
 };
 
 // Tap (jx, jy) of CF index cfi (fracu = cfi % os, fracv = (cfi / os) % os,
