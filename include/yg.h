@@ -233,6 +233,28 @@ int yg_mlp_loss_grad(const float* params, const float* x, const float* t, int64_
 /* y (n x 2) of the network with params rounded to FP16, host arrays */
 int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y);
 
+/* ---- major cycle as a CUDA graph ----
+ * The caller's major-cycle sequence of ImageFFTEquation::calcImagingEquations
+ * (ImageFFTEquation.cc:437-479) for n independent imaging instances: instance
+ * i degrids the model held by degridders[i] (after yg_initialise_degrid) into
+ * model visibilities, subtracts them from the observed visibilities of
+ * chunks[i] (device-resident, on_device = 1) and grids the residual with
+ * gridders[i] (after yg_initialise_grid).  yg_cycle_create bins every chunk,
+ * runs one cycle uncaptured (sizing every buffer) and records the n
+ * sequences, each on a branch of its own, into one CUDA graph; yg_cycle_run
+ * replays it `cycles` times.  Between runs the caller may load a new model
+ * (yg_initialise_degrid with an image of the same shape) and re-initialise
+ * the residual grids (yg_initialise_grid): buffers keep their addresses.
+ * The handles, chunks and arrays must outlive the cycle. */
+typedef struct yg_cycle yg_cycle;
+int yg_cycle_create(int32_t n, yg_gridder* const* degridders, yg_gridder* const* gridders, const yg_chunk* chunks,
+                    yg_cycle** out);
+/* replays the graph `cycles` times; *gpu_ms (may be NULL) receives the GPU time */
+int yg_cycle_run(yg_cycle* c, int32_t cycles, float* gpu_ms);
+/* nodes of the recorded graph */
+int yg_cycle_info(const yg_cycle* c, int64_t* nodes);
+void yg_cycle_destroy(yg_cycle* c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "../../include/yg.h"
+#include "yg_cycle.h"
 #include "yg_gridder.h"
 
 struct yg_gridder {
@@ -18,6 +19,10 @@ struct yg_gridder {
 
 struct yg_plan {
   yg::Plan pl;
+};
+
+struct yg_cycle {
+  yg::CycleBatch b;
 };
 
 namespace {
@@ -474,5 +479,39 @@ int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y) {
     if (n > 0) ck(cudaMemcpy(y, Y.p, n * 2 * sizeof(float), cudaMemcpyDeviceToHost));
   });
 }
+
+int yg_cycle_create(int32_t n, yg_gridder* const* degridders, yg_gridder* const* gridders, const yg_chunk* chunks,
+                    yg_cycle** out) {
+  return guarded([&] {
+    if (n <= 0 || !degridders || !gridders || !chunks || !out) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    std::vector<yg::Gridder*> dg(n), gg(n);
+    std::vector<yg::Chunk> ch(n);
+    for (int i = 0; i < n; ++i) {
+      dg[i] = &G(degridders[i]);
+      gg[i] = &G(gridders[i]);
+      ch[i] = to_chunk(&chunks[i]);
+    }
+    auto c = std::make_unique<yg_cycle>();
+    c->b.build(dg, gg, ch);
+    *out = c.release();
+  });
+}
+
+int yg_cycle_run(yg_cycle* c, int32_t cycles, float* gpu_ms) {
+  return guarded([&] {
+    if (!c || cycles < 0) throw yg::YgError{YG_ERR_ARG, "NULL cycle or negative count"};
+    const float ms = c->b.run(cycles);
+    if (gpu_ms) *gpu_ms = ms;
+  });
+}
+
+int yg_cycle_info(const yg_cycle* c, int64_t* nodes) {
+  return guarded([&] {
+    if (!c || !nodes) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    *nodes = c->b.nodes;
+  });
+}
+
+void yg_cycle_destroy(yg_cycle* c) { delete c; }
 
 }  // extern "C"

@@ -846,35 +846,47 @@ void Gridder::grid(const Chunk& c) {
   grid_plan(dc, pl);
 }
 
+// MFS weights of the chunk's channels on the device (null without MFS).
+const float* Gridder::mfs_weights(const Chunk& dc) {
+  if (!mfs_) return nullptr;
+  const std::vector<double> f = host_freqs(dc);
+  std::vector<float> w(dc.nchan);
+  for (int i = 0; i < dc.nchan; ++i) {
+    const double ratio = (f[i] - mfs_reffreq_) / mfs_reffreq_;
+    w[i] = mfs_order_ == 0 ? 1.0f : (mfs_order_ == 1 ? (float)ratio : (mfs_order_ == 2 ? (float)(ratio * ratio) : (float)std::pow(ratio, mfs_order_)));
+  }
+  cuda_check(mfs_d_.ensure(dc.nchan * sizeof(float)), "alloc");
+  cuda_check(cudaMemcpyAsync(mfs_d_.p, w.data(), dc.nchan * sizeof(float), cudaMemcpyHostToDevice, stream_), "up");
+  cuda_check(cudaStreamSynchronize(stream_), "up");
+  return mfs_d_.as<float>();
+}
+
+// The kernels of one grid pass over a plan, enqueued on st with no host
+// synchronisation and no allocation once the buffers have their size (the
+// part of grid_plan that a CUDA graph records).
+void Gridder::grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0,
+                           cudaEvent_t k1) {
+  VisArgs v = vis_args(dc, mfs, psf_);
+  const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
+  const LearnedCF lcf = learned_view_for(dc, const_cast<Plan&>(pl));
+  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
+                     err_.as<DevError>(), st, k0, k1, grid_mode_, cf_form_ != 0 ? &lcf : nullptr),
+           "gridding");
+  rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), st), "carry");
+}
+
 void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
   throw_if(!grids_.p || nx_ == 0, YG_ERR_STATE, "initialiseGrid must be called before grid");
   if (kind_ != Kind::AWProject) build_cf();
   throw_if(!cf_built_, YG_ERR_STATE, "convolution functions are not built");
-  const float* mfs = nullptr;
-  if (mfs_) {
-    const std::vector<double> f = host_freqs(dc);
-    std::vector<float> w(dc.nchan);
-    for (int i = 0; i < dc.nchan; ++i) {
-      const double ratio = (f[i] - mfs_reffreq_) / mfs_reffreq_;
-      w[i] = mfs_order_ == 0 ? 1.0f : (mfs_order_ == 1 ? (float)ratio : (mfs_order_ == 2 ? (float)(ratio * ratio) : (float)std::pow(ratio, mfs_order_)));
-    }
-    cuda_check(mfs_d_.ensure(dc.nchan * sizeof(float)), "alloc");
-    cuda_check(cudaMemcpyAsync(mfs_d_.p, w.data(), dc.nchan * sizeof(float), cudaMemcpyHostToDevice, stream_), "up");
-    mfs = mfs_d_.as<float>();
-  }
-  VisArgs v = vis_args(dc, mfs, psf_);
+  const float* mfs = mfs_weights(dc);
   cudaEvent_t e0, e1, k0, k1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventCreate(&k0);
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
-  const LearnedCF lcf = learned_view_for(dc, const_cast<Plan&>(pl));
-  rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
-                     err_.as<DevError>(), stream_, k0, k1, grid_mode_, cf_form_ != 0 ? &lcf : nullptr),
-           "gridding");
-  rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), stream_), "carry");
+  grid_enqueue(dc, pl, mfs, stream_, k0, k1);
   cudaEventRecord(e1, stream_);
   check_error();
   float ms = 0, kms = 0;
@@ -912,33 +924,28 @@ void Gridder::degrid(Chunk& c) {
   }
 }
 
+// The kernels of one degrid pass over a plan on st (see grid_enqueue).
+void Gridder::degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0,
+                             cudaEvent_t k1) {
+  VisArgs v = vis_args(dc, mfs, false);
+  const LearnedCF lcf = learned_view_for(dc, pl);
+  rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
+                       carry_.as<float2>(), err_.as<DevError>(), st, k0, k1, cf_form_ != 0 ? &lcf : nullptr),
+           "degridding");
+}
+
 void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
   throw_if(!grids_.p || nx_ == 0, YG_ERR_STATE, "initialiseDegrid must be called before degrid");
   if (kind_ != Kind::AWProject) build_cf();
   throw_if(!cf_built_, YG_ERR_STATE, "convolution functions are not built");
-  const float* mfs = nullptr;
-  if (mfs_) {
-    const std::vector<double> f = host_freqs(dc);
-    std::vector<float> w(dc.nchan);
-    for (int i = 0; i < dc.nchan; ++i) {
-      const double ratio = (f[i] - mfs_reffreq_) / mfs_reffreq_;
-      w[i] = mfs_order_ == 0 ? 1.0f : (mfs_order_ == 1 ? (float)ratio : (mfs_order_ == 2 ? (float)(ratio * ratio) : (float)std::pow(ratio, mfs_order_)));
-    }
-    cuda_check(mfs_d_.ensure(dc.nchan * sizeof(float)), "alloc");
-    cuda_check(cudaMemcpyAsync(mfs_d_.p, w.data(), dc.nchan * sizeof(float), cudaMemcpyHostToDevice, stream_), "up");
-    mfs = mfs_d_.as<float>();
-  }
-  VisArgs v = vis_args(dc, mfs, false);
+  const float* mfs = mfs_weights(dc);
   cudaEvent_t e0, e1, k0, k1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventCreate(&k0);
   cudaEventCreate(&k1);
   cudaEventRecord(e0, stream_);
-  const LearnedCF lcf = learned_view_for(dc, pl);
-  rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
-                       carry_.as<float2>(), err_.as<DevError>(), stream_, k0, k1, cf_form_ != 0 ? &lcf : nullptr),
-           "degridding");
+  degrid_enqueue(dc, pl, mfs, stream_, k0, k1);
   cudaEventRecord(e1, stream_);
   check_error();
   float ms = 0, kms = 0;

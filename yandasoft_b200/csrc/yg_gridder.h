@@ -111,6 +111,14 @@ class Gridder {
   void bin(const Chunk& c, Plan& pl);
   void grid_plan(const Chunk& c, const Plan& pl);
   void degrid_plan(Chunk& c, Plan& pl);
+  // launch-only cores of grid_plan / degrid_plan: no host synchronisation,
+  // no allocation once sized, any stream (what a CUDA graph records)
+  void grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
+                    cudaEvent_t k1 = nullptr);
+  void degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
+                      cudaEvent_t k1 = nullptr);
+  const float* mfs_weights(const Chunk& dc);
+  void check_device_error() { check_error(); }
   void set_tile(int t) { tile_override_ = t; }
   void set_grid_mode(int m) { grid_mode_ = m; }
   int tile_for(int smax, int npol) const;

@@ -38,6 +38,7 @@ EXPORTS = [
     "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
     "yg_set_grid_variant", "yg_degrid_noalloc", "yg_mlp_nparams", "yg_learned_train", "yg_set_cf_form",
     "yg_learned_get_params", "yg_learned_set_params", "yg_mlp_loss_grad", "yg_mlp_eval",
+    "yg_cycle_create", "yg_cycle_run", "yg_cycle_info", "yg_cycle_destroy",
 ]
 
 
@@ -125,6 +126,12 @@ def load(path: str | None = None):
     L.yg_learned_set_params.argtypes = [P, P, ctypes.c_float]
     L.yg_mlp_loss_grad.argtypes = [P, P, P, I64, ctypes.c_float, P, ctypes.POINTER(D)]
     L.yg_mlp_eval.argtypes = [P, P, I64, P]
+    L.yg_cycle_create.argtypes = [I32, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(yg_chunk),
+                                  ctypes.POINTER(P)]
+    L.yg_cycle_run.argtypes = [P, I32, ctypes.POINTER(ctypes.c_float)]
+    L.yg_cycle_info.argtypes = [P, ctypes.POINTER(I64)]
+    L.yg_cycle_destroy.argtypes = [P]
+    L.yg_cycle_destroy.restype = None
     _LIB = L
     return L
 
@@ -455,6 +462,43 @@ class IVisGridder:
         keys = ["samples_gridded", "taps_gridded", "samples_degridded", "taps_degridded", "ms_grid", "ms_degrid",
                 "ms_cf", "cf_planes"]
         return dict(zip(keys, out.tolist()))
+
+
+class MajorCycle:
+    """degrid -> subtract -> grid for n instances, recorded once as one CUDA
+    graph (each instance on a branch of its own) and replayed per cycle.
+    degridders[i] holds the model (initialiseDegrid), gridders[i] receives the
+    residual (initialiseGrid), accessors[i] are device-resident observed
+    chunks.  See yg_cycle_create."""
+
+    def __init__(self, degridders, gridders, accessors):
+        self._lib = load()
+        n = len(degridders)
+        if not (len(gridders) == n == len(accessors)):
+            raise AskapError(1, "one degridder, gridder and accessor per instance")
+        self._keep = (list(degridders), list(gridders), list(accessors))
+        dg = (P * n)(*[g.h for g in degridders])
+        gg = (P * n)(*[g.h for g in gridders])
+        ch = (yg_chunk * n)(*[a.c() for a in accessors])
+        self._arrays = (dg, gg, ch)
+        self.h = P()
+        _check(self._lib.yg_cycle_create(n, dg, gg, ch, ctypes.byref(self.h)))
+
+    def run(self, cycles=1) -> float:
+        """Replays the graph `cycles` times; returns the GPU milliseconds."""
+        ms = ctypes.c_float()
+        _check(self._lib.yg_cycle_run(self.h, int(cycles), ctypes.byref(ms)))
+        return ms.value
+
+    def nodes(self) -> int:
+        n = I64()
+        _check(self._lib.yg_cycle_info(self.h, ctypes.byref(n)))
+        return n.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            self._lib.yg_cycle_destroy(self.h)
+            self.h = P()
 
 
 def mlp_nparams() -> int:
