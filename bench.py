@@ -49,7 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 3],
+                    help="0, 1: one instance; 3: 64 uneven instances, major cycles as one CUDA graph")
+    ap.add_argument("--instances", type=int, default=64, help="config 3: number of imaging instances")
+    ap.add_argument("--cycles", type=int, default=5, help="config 3: major cycles timed")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
@@ -640,8 +643,89 @@ def run_reference(args, w):
     print(json.dumps(line))
 
 
+def batch_instances(n, seed=7, scale=1.0):
+    """Config 3: n imaging instances generated as config 0 (36 antennas in a
+    6 km disk, WProject, 20 sources, noise 0.01) with their own seeds, grid
+    sizes drawn from {512, 1024, 2048, 4096}^2 (field of view 1.1-4.6 deg),
+    visibility counts log-uniform in [1e5, 5e7] and 1-32 channels."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = int(rng.choice([512, 1024, 2048, 4096]))
+        nvis = float(np.exp(rng.uniform(math.log(1e5), math.log(5e7)))) * scale
+        nchan = int(rng.integers(1, 33))
+        ntime = max(1, int(round(nvis / (630 * nchan))))
+        w = workload(0)
+        w.update(name="instance%02d" % i, nx=nx, cell=8.0 if nx <= 2048 else 4.0, nchan=nchan, duration=ntime * 10.0,
+                 seed=1000 + i, nwplanes=33)
+        out.append(w)
+    return out
+
+
+def run_batch(args):
+    """Config 3: `instances` independent imaging instances, each a degridder
+    with its model and a gridder for the residual over a device-resident
+    chunk, recorded as one CUDA graph (yandasoft_b200.gridder.MajorCycle) and
+    replayed for `cycles` major cycles.  value = visibility samples degridded
+    and gridded per second over all instances and cycles."""
+    import torch
+    from yandasoft_b200 import build
+    from yandasoft_b200 import gridder as G
+    build.build()
+    G.load()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ws = batch_instances(args.instances, scale=args.scale)
+    t0 = time.perf_counter()
+    insts, dgs, ggs, accs, nvis, shapes = [], [], [], [], 0, []
+    for w in ws:
+        d = gen_device(w)
+        ps = parset_for(w, d["wmax"])
+        cell = w["cell"] * ARCSEC
+        axes = G.Axes(cell, cell)
+        nx = w["nx"]
+        acc = G.Accessor(d["uvw"], d["freq"], d["vis"], shape=(d["nrow"], d["nchan"], d["npol"]))
+        gd = G.VisGridderFactory.make(ps)
+        gd.initialiseDegrid(axes, model_image(w, d["sky"], d["npol"]))
+        gg = G.VisGridderFactory.make(ps)
+        gg.initialiseGrid(axes, (nx, nx, d["npol"], 1))
+        insts.append(d)
+        dgs.append(gd)
+        ggs.append(gg)
+        accs.append(acc)
+        nvis += d["nrow"] * d["nchan"] * d["npol"]
+        shapes.append((nx, int(d["nrow"] * d["nchan"])))
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cyc = G.MajorCycle(dgs, ggs, accs)
+    t_build = time.perf_counter() - t0
+    supports = sorted({g.support()[0] for g in ggs})
+    cyc.run(1)                                   # warm replay
+    with ClockSampler(0) as clk:
+        ms = cyc.run(args.cycles)
+    launches = G.kernel_launch_count()
+    line = {
+        "metric": "major-cycle degrid+subtract+grid Mvis/s over %d instances on 1 B200 (one CUDA graph)"
+                  % len(ws),
+        "value": round(nvis * args.cycles / (ms / 1e3) / 1e6, 3), "unit": "Mvis/s", "n_gpus": 1,
+        "steps": args.cycles, "warmup": 1, "ms_per_step": round(ms / args.cycles, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded per instance)",
+        "config": {"workload": "config3_batched_major_cycle", "instances": len(ws), "vis_samples": int(nvis),
+                   "grid_sizes": sorted({s[0] for s in shapes}), "supports": supports,
+                   "graph_nodes": cyc.nodes(), "setup_s": round(t_build, 2), "generate_s": round(t_gen, 2),
+                   "step": "one major cycle: every instance degrids its model, subtracts, grids the residual"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(cyc.nodes() * args.cycles),
+        "gpu_launches_note": "graph nodes (kernels and memsets) x cycles",
+    }
+    del launches
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.config == 3:
+        run_batch(args)
+        return
     w = workload(args.config, args.scale)
     if args.impl == "reference":
         run_reference(args, w)

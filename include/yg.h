@@ -255,6 +255,24 @@ int yg_cycle_run(yg_cycle* c, int32_t cycles, float* gpu_ms);
 int yg_cycle_info(const yg_cycle* c, int64_t* nodes);
 void yg_cycle_destroy(yg_cycle* c);
 
+/* ---- autotuner ----
+ * No counterpart in the reference.  Times a degrid + grid pass over a
+ * device-resident chunk for up to max_trials candidates of (uv tile side,
+ * samples per work item, k_grid thread layout) and keeps the fastest for this
+ * handle and, process-wide, for every later handle whose CFs have the same
+ * padded width and polarisation count.  The handle must be initialised
+ * (yg_initialise_grid or yg_initialise_degrid); its grids hold extra passes
+ * afterwards, so re-initialise before real use. */
+typedef struct {
+  int32_t tile, items, variant;   /* the choice kept */
+  int32_t trials;                 /* candidates timed */
+  float best_ms, default_ms;      /* degrid + grid pass with the choice / with the defaults */
+  int32_t cf_width, npol;         /* the class it is kept for (padded CF width) */
+} yg_tune_report;
+int yg_autotune(yg_gridder* g, const yg_chunk* chunk, int32_t max_trials, yg_tune_report* rep);
+/* forgets every process-wide choice */
+void yg_autotune_reset(void);
+
 #ifdef __cplusplus
 }
 #endif

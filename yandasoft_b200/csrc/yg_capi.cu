@@ -514,4 +514,24 @@ int yg_cycle_info(const yg_cycle* c, int64_t* nodes) {
 
 void yg_cycle_destroy(yg_cycle* c) { delete c; }
 
+int yg_autotune(yg_gridder* g, const yg_chunk* chunk, int32_t max_trials, yg_tune_report* rep) {
+  return guarded([&] {
+    if (!chunk || max_trials < 1) throw yg::YgError{YG_ERR_ARG, "chunk and a positive trial count are required"};
+    yg::Chunk c = to_chunk(chunk);
+    const yg::TuneReport r = G(g).autotune(c, max_trials);
+    if (rep) {
+      rep->tile = r.best.tile;
+      rep->items = r.best.vmax;
+      rep->variant = r.best.variant;
+      rep->trials = (int32_t)r.trials.size();
+      rep->best_ms = r.best_ms;
+      rep->default_ms = r.default_ms;
+      rep->cf_width = r.wpad;
+      rep->npol = r.npol;
+    }
+  });
+}
+
+void yg_autotune_reset(void) { yg::tune_clear(); }
+
 }  // extern "C"

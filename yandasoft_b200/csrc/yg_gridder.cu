@@ -705,8 +705,20 @@ void Gridder::init_cf(const Chunk& dc) {
 // ---------------------------------------------------------------------------
 // binning
 // ---------------------------------------------------------------------------
+// the k_grid thread layout: the caller's, else the autotuner's for this CF
+// width class, else the default
+int Gridder::grid_variant() const {
+  if (grid_mode_ > 0) return grid_mode_;
+  TuneChoice c;
+  const int smax = (cf_.maxsize - 1) / 2;
+  if (tune_lookup(((2 * smax + 1) + 15) / 16 * 16, npol_, &c)) return c.variant;
+  return 0;
+}
+
 int Gridder::tile_for(int smax, int npol) const {
   if (tile_override_ > 0) return tile_override_;
+  TuneChoice c;
+  if (tune_lookup(((2 * smax + 1) + 15) / 16 * 16, npol, &c) && c.tile > 0) return c.tile;
   return grid_tile_for(smax, npol, cf_.view().varsup != 0);
 }
 
@@ -808,6 +820,10 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
   fill_bin_args(a, dc, pl.chanmap.as<int>(), row_ok);
   // samples per work item: enough items for ~8 per SM, never below 512
   int vmax = vmax_;
+  TuneChoice tc;
+  const int smax_b = (cf_.maxsize - 1) / 2;
+  const bool tuned = tune_lookup(((2 * smax_b + 1) + 15) / 16 * 16, npol_, &tc);
+  if (vmax <= 0 && tuned && tile_override_ <= 0) vmax = tc.vmax;
   if (vmax <= 0) {
     const long long n = dc.nrow * (long long)dc.nchan;
     vmax = (int)std::min<long long>(1 << 20, std::max<long long>(512, n / (148 * 8)));
@@ -870,7 +886,7 @@ void Gridder::grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cu
   const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
   const LearnedCF lcf = learned_view_for(dc, const_cast<Plan&>(pl));
   rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
-                     err_.as<DevError>(), st, k0, k1, grid_mode_, cf_form_ != 0 ? &lcf : nullptr),
+                     err_.as<DevError>(), st, k0, k1, grid_variant(), cf_form_ != 0 ? &lcf : nullptr),
            "gridding");
   rc_check(plan_grid_carry(const_cast<Plan&>(pl), v, carry_.as<float2>(), st), "carry");
 }

@@ -70,6 +70,24 @@ struct Stats {
   double kgrid_calls = 0, kdegrid_calls = 0;
 };
 
+// autotuner (yg_autotune.cu)
+struct TuneChoice {
+  int tile = 0, vmax = 0, variant = 0;
+};
+struct TuneTrial {
+  int tile, vmax, variant;
+  float ms;        // degrid + grid pass; < 0: the candidate does not fit
+};
+struct TuneReport {
+  int wpad = 0, npol = 0;
+  TuneChoice best;
+  float best_ms = -1.f, default_ms = -1.f;
+  std::vector<TuneTrial> trials;
+};
+bool tune_lookup(int wpad, int npol, TuneChoice* out);
+void tune_store(int wpad, int npol, const TuneChoice& c);
+void tune_clear();
+
 class Gridder {
  public:
   // VisGridderFactory::make
@@ -118,10 +136,17 @@ class Gridder {
   void degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
                       cudaEvent_t k1 = nullptr);
   const float* mfs_weights(const Chunk& dc);
+  TuneReport autotune(const Chunk& dc, int max_trials);
+  void apply_tuning(const TuneChoice& c) {
+    tile_override_ = c.tile;
+    vmax_ = c.vmax;
+    grid_mode_ = c.variant;
+  }
   void check_device_error() { check_error(); }
   void set_tile(int t) { tile_override_ = t; }
   void set_grid_mode(int m) { grid_mode_ = m; }
   int tile_for(int smax, int npol) const;
+  int grid_variant() const;
   int items_vmax() const { return vmax_; }
   void set_vmax(int v) { vmax_ = v; }
   void sync();

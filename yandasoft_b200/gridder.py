@@ -38,7 +38,7 @@ EXPORTS = [
     "yg_synchronize", "yg_get_stream", "yg_get_kernel_times", "yg_kernel_launch_count",
     "yg_set_grid_variant", "yg_degrid_noalloc", "yg_mlp_nparams", "yg_learned_train", "yg_set_cf_form",
     "yg_learned_get_params", "yg_learned_set_params", "yg_mlp_loss_grad", "yg_mlp_eval",
-    "yg_cycle_create", "yg_cycle_run", "yg_cycle_info", "yg_cycle_destroy",
+    "yg_cycle_create", "yg_cycle_run", "yg_cycle_info", "yg_cycle_destroy", "yg_autotune", "yg_autotune_reset",
 ]
 
 
@@ -63,6 +63,11 @@ class yg_learn_params(ctypes.Structure):
 class yg_learn_report(ctypes.Structure):
     _fields_ = [("final_loss", D), ("train_ms", ctypes.c_float), ("steps", I32), ("scale", ctypes.c_float),
                 ("cf_table_bytes", D), ("network_bytes", D)]
+
+
+class yg_tune_report(ctypes.Structure):
+    _fields_ = [("tile", I32), ("items", I32), ("variant", I32), ("trials", I32), ("best_ms", ctypes.c_float),
+                ("default_ms", ctypes.c_float), ("cf_width", I32), ("npol", I32)]
 
 
 class yg_chunk(ctypes.Structure):
@@ -132,6 +137,9 @@ def load(path: str | None = None):
     L.yg_cycle_info.argtypes = [P, ctypes.POINTER(I64)]
     L.yg_cycle_destroy.argtypes = [P]
     L.yg_cycle_destroy.restype = None
+    L.yg_autotune.argtypes = [P, ctypes.POINTER(yg_chunk), I32, ctypes.POINTER(yg_tune_report)]
+    L.yg_autotune_reset.argtypes = []
+    L.yg_autotune_reset.restype = None
     _LIB = L
     return L
 
@@ -368,6 +376,15 @@ class IVisGridder:
         p = np.ascontiguousarray(params, dtype=np.float32)
         _check(self._lib.yg_learned_set_params(self.h, p.ctypes.data, float(scale)))
 
+    # ---- autotuner (no counterpart in the reference) ----
+    def autotune(self, acc: Accessor, max_trials=12):
+        """Times (tile, samples per item, thread layout) candidates on a
+        device-resident chunk; keeps the fastest for this CF width class."""
+        c = acc.c()
+        r = yg_tune_report()
+        _check(self._lib.yg_autotune(self.h, ctypes.byref(c), int(max_trials), ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in yg_tune_report._fields_}
+
     # ---- plans (repeated passes over resident data) ----
     def plan(self, acc: Accessor) -> Plan:
         return Plan(self, acc)
@@ -499,6 +516,11 @@ class MajorCycle:
         if getattr(self, "h", None) and self.h.value:
             self._lib.yg_cycle_destroy(self.h)
             self.h = P()
+
+
+def autotune_reset():
+    """Forgets every process-wide autotuner choice."""
+    load().yg_autotune_reset()
 
 
 def mlp_nparams() -> int:
