@@ -338,16 +338,15 @@ def run_b200(args, w):
     acc_model = G.Accessor(d["uvw"], d["freq"], model_buf, shape=(d["nrow"], d["nchan"], npol))
     tune = None
     if not args.no_tune and not args.tile and not args.variant:
-        # the autotuner on the first 5% of the track; its choice serves every gridder of this CF width
-        nr = max(1, d["nrow"] // 20)
-        tacc = G.Accessor(d["uvw"][:nr].contiguous(), d["freq"], d["vis"][:, :, :nr].contiguous(),
-                          shape=(nr, d["nchan"], npol))
+        # the autotuner on the workload itself (sample density per tile sets the
+        # optimum); its choice serves every gridder of this CF width
         tuner = G.VisGridderFactory.make(ps)
         tuner.initialiseGrid(axes, (nx, nx, npol, 1))
         t0 = time.perf_counter()
-        tune = tuner.autotune(tacc, max_trials=12)
+        tune = tuner.autotune(acc, max_trials=10)
         tune["seconds"] = round(time.perf_counter() - t0, 2)
-        del tuner, tacc
+        del tuner
+        torch.cuda.empty_cache()
     gg = G.VisGridderFactory.make(ps)
     if args.tile:
         gg.set_tile(args.tile)

@@ -86,49 +86,51 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   ck(cudaEventCreate(&e0), "event");
   ck(cudaEventCreate(&e1), "event");
   int trials = 0;
-  for (int v : variants) {
-    for (int t : tiles) {
-      for (int vm : vmaxes) {
-        if (trials >= max_trials) break;
-        // the default first: every later candidate must beat it
-        tile_override_ = t;
-        vmax_ = vm;
-        grid_mode_ = v;
-        float ms = -1.f;
-        try {
-          Plan pl;
-          bin(dc, pl);
-          ck(cudaMemsetAsync(model.p, 0, bytes, stream_), "clear");
-          degrid_enqueue(scratch_chunk, pl, mfs, stream_);
-          grid_enqueue(dc, pl, mfs, stream_);
-          check_error();
-          ck(cudaEventRecord(e0, stream_), "event");
-          degrid_enqueue(scratch_chunk, pl, mfs, stream_);
-          grid_enqueue(dc, pl, mfs, stream_);
-          ck(cudaEventRecord(e1, stream_), "event");
-          ck(cudaEventSynchronize(e1), "trial");
-          check_error();
-          cudaEventElapsedTime(&ms, e0, e1);
-        } catch (const YgError& e) {
-          if (e.code != YG_ERR_UNSUPPORTED) {
-            tile_override_ = save_tile;
-            vmax_ = save_vmax;
-            grid_mode_ = save_mode;
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            throw;
-          }
-        }
-        ++trials;
-        rep.trials.push_back(TuneTrial{t, vm, v, ms});
-        if (ms > 0.f && (rep.best_ms < 0.f || ms < rep.best_ms)) {
-          rep.best_ms = ms;
-          rep.best = TuneChoice{t, vm, v};
-        }
-        if (t == def_tile && vm == def_vmax && v == 1) rep.default_ms = ms;
+  auto trial = [&](int t, int vm, int v) {
+    tile_override_ = t;
+    vmax_ = vm;
+    grid_mode_ = v;
+    float ms = -1.f;
+    try {
+      Plan pl;
+      bin(dc, pl);
+      ck(cudaMemsetAsync(model.p, 0, bytes, stream_), "clear");
+      degrid_enqueue(scratch_chunk, pl, mfs, stream_);
+      grid_enqueue(dc, pl, mfs, stream_);
+      check_error();
+      ck(cudaEventRecord(e0, stream_), "event");
+      degrid_enqueue(scratch_chunk, pl, mfs, stream_);
+      grid_enqueue(dc, pl, mfs, stream_);
+      ck(cudaEventRecord(e1, stream_), "event");
+      ck(cudaEventSynchronize(e1), "trial");
+      check_error();
+      cudaEventElapsedTime(&ms, e0, e1);
+    } catch (const YgError& e) {
+      if (e.code != YG_ERR_UNSUPPORTED) {
+        tile_override_ = save_tile;
+        vmax_ = save_vmax;
+        grid_mode_ = save_mode;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
       }
     }
-  }
+    ++trials;
+    rep.trials.push_back(TuneTrial{t, vm, v, ms});
+    if (ms > 0.f && (rep.best_ms < 0.f || ms < rep.best_ms)) {
+      rep.best_ms = ms;
+      rep.best = TuneChoice{t, vm, v};
+    }
+    if (t == def_tile && vm == def_vmax && v == 1) rep.default_ms = ms;
+  };
+  // first the tile and the thread layout at the default work-item size (the
+  // default itself first), then the work-item size around the best of those
+  for (int v : variants)
+    for (int t : tiles)
+      if (trials < max_trials) trial(t, def_vmax, v);
+  const TuneChoice lead = rep.best;
+  for (int vm : vmaxes)
+    if (vm != def_vmax && trials < max_trials && lead.tile > 0) trial(lead.tile, vm, lead.variant);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   tile_override_ = save_tile;

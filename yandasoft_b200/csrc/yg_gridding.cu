@@ -522,7 +522,6 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
     // x residue t mod Wp and the y residues t / Wp + RSTEP * q, so the x part
     // of the index arithmetic is done once per sample and the slots step down
     // the rows.
-    const int trash = Pg * Pg + threadIdx.x;     // target of slots beyond Wp^2
     int rx[RSTEP ? 1 : MAXSLOTS], rowoff[RSTEP ? 1 : MAXSLOTS];
     bool live[RSTEP ? 1 : MAXSLOTS];
     if (RSTEP) {
@@ -539,6 +538,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
       }
     }
     const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
+    const int trash = Pg * Pg + threadIdx.x;     // target of slots beyond Wp^2
     int cur_cfi = -1;
     for (int nseg_done = 0;; ++nseg_done) {
       const int stage = nseg_done % NST;
@@ -578,13 +578,21 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
           int cell = cb + jx + Pg * jy0;
           int tap = jx + Wp * jy0;
           const int lim = Wp - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
+          // taps of the padding hold zeros and are accumulated like the others:
+          // predicating them off costs more than it saves.  The network is
+          // evaluated only inside the CF width.
 #pragma unroll
           for (int q = 0; q < MAXSLOTS; ++q) {
             const bool wrap = RSTEP * q >= lim;
             const int c2 = wrap ? cell - PgW : cell;
             const int t2 = wrap ? tap - Wp2 : tap;
-            const float2 c = CFM == 3 ? mlp_tap_exact(ws, a.lcf, r.z, t2 % Wp, t2 / Wp, wcf, xe)
-                                      : (CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2]);
+            float2 c;
+            if (CFM == 3) {
+              const int row = wrap ? jy0 + RSTEP * q - Wp : jy0 + RSTEP * q;
+              c = (jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe) : make_float2(0.f, 0.f);
+            } else {
+              c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
+            }
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               float2 g = acc_s[p * PG2 + c2];
@@ -604,7 +612,8 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
             const int tq = live[q] ? jx + Wp * jy : 0;
-            const float2 c = CFM == 3 ? (live[q] ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe) : make_float2(0.f, 0.f))
+            const float2 c = CFM == 3 ? ((live[q] && jx < wcf && jy < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe)
+                                                                           : make_float2(0.f, 0.f))
                                       : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
@@ -1113,11 +1122,17 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
           for (int p = 0; p < NPOL; ++p) re[u][p] = im[u][p] = 0.f;
         int tap = lane;
         int jx = jx0;
+        int row = jy0;
         int cell = origin + jx0 + Pg * jy0;
         for (int st = 0; st < steps; st += 4) {
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const float2 cv = CFM == 3 ? mlp_tap_exact(ws, a.lcf, r.z, tap % Wp, tap / Wp, wcf, xe) : cf_s[tap];
+            // taps of the padding hold zeros in the table (read unconditionally,
+            // which keeps the four partial sums' loads independent); the
+            // network is evaluated only inside the CF width
+            const float2 cv = CFM == 3 ? ((jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe)
+                                                                   : make_float2(0.f, 0.f))
+                                       : cf_s[tap];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
               const float2 g = g_s[p * PG2 + cell];
@@ -1127,10 +1142,12 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
             tap += 32;
             if (rows_per_step) {
               cell += rows_per_step * Pg;
+              row += rows_per_step;
             } else {
               jx += 32;
               const bool wrap = jx >= Wp;
               jx = wrap ? jx - Wp : jx;
+              row += wrap ? 1 : 0;
               cell += wrap ? 32 - Wp + Pg : 32;
             }
           }
