@@ -384,6 +384,12 @@ std::unique_ptr<Gridder> Gridder::clone() const {
 }
 
 Gridder::~Gridder() {
+  if (copy_stream_) {
+    cudaStreamSynchronize(copy_stream_);
+    cudaStreamDestroy(copy_stream_);
+  }
+  for (auto& e : piece_up_)
+    if (e) cudaEventDestroy(e);
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
@@ -850,9 +856,98 @@ static VisArgs vis_args(const Chunk& dc, const float* mfs, bool psf) {
 // ---------------------------------------------------------------------------
 // grid / degrid
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// host chunks in row pieces: the next piece's upload (a copy stream) overlaps
+// the binning and gridding of the current one; degridded pieces go back to
+// the host while the next is degridded.  Row order is kept, so the result is
+// that of one call (sums of weights, the carried value of off-grid samples).
+// ---------------------------------------------------------------------------
+bool Gridder::pipelined(const Chunk& c) const {
+  const double bytes = (double)c.nrow * c.nchan * c.npol * sizeof(float2);
+  return !c.on_device && kind_ != Kind::AWProject && !psf_ && bytes >= kPipeMinBytes && c.nrow >= 16;
+}
+
+Chunk Gridder::stage_rows(const Chunk& c, long long r0, long long nr, int b, bool need_vis) {
+  Staging& s = staging_[b];
+  cudaStream_t cs = copy_stream_;
+  const size_t nrows = (size_t)nr;
+  const size_t planes = (size_t)c.nchan * c.npol;
+  auto up = [&](DevBuf& d, const void* src, size_t bytes) -> void* {
+    if (!src) return nullptr;
+    cuda_check(d.ensure(bytes), "alloc upload");
+    cuda_check(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, cs), "upload");
+    return d.p;
+  };
+  auto up2 = [&](DevBuf& d, const void* src, size_t elem) -> void* {
+    if (!src) return nullptr;
+    cuda_check(d.ensure(nrows * planes * elem), "alloc upload");
+    cuda_check(cudaMemcpy2DAsync(d.p, nrows * elem, (const char*)src + r0 * elem, (size_t)c.nrow * elem,
+                                 nrows * elem, planes, cudaMemcpyHostToDevice, cs),
+               "upload rows");
+    return d.p;
+  };
+  Chunk dc = c;
+  dc.nrow = nr;
+  dc.uvw = (const double*)up(s.uvw, c.uvw + 3 * r0, nrows * 3 * sizeof(double));
+  dc.delay = c.delay ? (const double*)up(s.delay, c.delay + r0, nrows * sizeof(double)) : nullptr;
+  dc.freq = (const double*)up(s.freq, c.freq, (size_t)c.nchan * sizeof(double));
+  dc.vis = need_vis ? (float2*)up2(s.vis, c.vis, sizeof(float2)) : nullptr;
+  dc.noise = (const float2*)up2(s.noise, c.noise, sizeof(float2));
+  dc.flag = (const uint8_t*)up2(s.flag, c.flag, 1);
+  dc.feed1 = c.feed1 ? (const int*)up(s.feed, c.feed1 + r0, nrows * sizeof(int)) : nullptr;
+  dc.pointing = c.pointing ? c.pointing + 2 * r0 : nullptr;
+  dc.on_device = 1;
+  if (!piece_up_[b]) cuda_check(cudaEventCreateWithFlags(&piece_up_[b], cudaEventDisableTiming), "event");
+  cuda_check(cudaEventRecord(piece_up_[b], cs), "event");
+  return dc;
+}
+
+void Gridder::run_pieces(Chunk& c, bool degridding) {
+  if (!copy_stream_) cuda_check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "stream");
+  const double bytes = (double)c.nrow * c.nchan * c.npol * sizeof(float2);
+  const int K = (int)std::max(2.0, std::min(16.0, std::ceil(bytes / kPipePieceBytes)));
+  const long long rows = (c.nrow + K - 1) / K;
+  const int npieces = (int)((c.nrow + rows - 1) / rows);
+  std::vector<Chunk> staged(2);
+  staged[0] = stage_rows(c, 0, std::min(rows, c.nrow), 0, true);
+  for (int k = 0; k < npieces; ++k) {
+    const int b = k & 1;
+    const long long r0 = k * rows, nr = std::min(rows, c.nrow - r0);
+    if (k + 1 < npieces) {
+      // buffer b ^ 1 was last used by piece k - 1, which has finished (the
+      // passes below end on a host synchronisation); a degridded piece's
+      // download was queued on the copy stream before this upload
+      const long long r1 = (k + 1) * rows;
+      staged[b ^ 1] = stage_rows(c, r1, std::min(rows, c.nrow - r1), b ^ 1, true);
+    }
+    // the host waits for this piece's upload (binning reads its frequencies
+    // through a synchronous copy); the next piece's upload runs on
+    cuda_check(cudaEventSynchronize(piece_up_[b]), "wait upload");
+    Chunk& dc = staged[b];
+    init_cf(dc);
+    bin(dc, piece_plan_[b]);
+    if (degridding) {
+      degrid_plan(dc, piece_plan_[b]);
+      cuda_check(cudaMemcpy2DAsync((char*)c.vis + r0 * sizeof(float2), (size_t)c.nrow * sizeof(float2), dc.vis,
+                                   (size_t)nr * sizeof(float2), (size_t)nr * sizeof(float2),
+                                   (size_t)c.nchan * c.npol, cudaMemcpyDeviceToHost, copy_stream_),
+                 "download rows");
+    } else {
+      grid_plan(dc, piece_plan_[b]);
+    }
+  }
+  cuda_check(cudaStreamSynchronize(copy_stream_), "pieces");
+}
+
 void Gridder::grid(const Chunk& c) {
   throw_if(nx_ == 0 || !grids_.p, YG_ERR_STATE, "initialiseGrid must be called before grid");
   throw_if(!sumw_.p, YG_ERR_STATE, "SumWeights not yet initialised");
+  if (pipelined(c)) {
+    ensure_device();
+    Chunk cc = c;
+    run_pieces(cc, false);
+    return;
+  }
   Chunk dc;
   upload_chunk(c, dc, !psf_, false);
   if (!c.on_device) dc.pointing = c.pointing;
@@ -926,6 +1021,11 @@ void Gridder::degrid(Chunk& c) {
   throw_if(psf_, YG_ERR_STATE, "the gridder is not supposed to be used for degridding in the PSF mode");
   if (model_empty_) return;
   throw_if(nx_ == 0 || !grids_.p, YG_ERR_STATE, "initialiseDegrid must be called before degrid");
+  if (pipelined(c)) {
+    ensure_device();
+    run_pieces(c, true);
+    return;
+  }
   Chunk dc;
   upload_chunk(c, dc, true, true);
   if (!c.on_device) dc.pointing = c.pointing;

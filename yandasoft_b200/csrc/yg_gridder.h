@@ -244,6 +244,19 @@ class Gridder {
   DevBuf scratch_, svis_, tmpvals_, cfwork_, img_tmp_, mfs_d_;
   int nsumw_rows_ = 1;
   Plan plan_;
+  // host chunks in row pieces (upload / download overlapping the passes)
+  struct Staging {
+    DevBuf uvw, delay, freq, vis, noise, flag, feed;
+  };
+  static constexpr double kPipeMinBytes = 256.0 * (1 << 20);   // smaller chunks go in one piece
+  static constexpr double kPipePieceBytes = 1024.0 * (1 << 20);
+  Staging staging_[2];
+  Plan piece_plan_[2];
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t piece_up_[2] = {nullptr, nullptr};
+  bool pipelined(const Chunk& c) const;
+  Chunk stage_rows(const Chunk& c, long long r0, long long nr, int b, bool need_vis);
+  void run_pieces(Chunk& c, bool degridding);
   ImageFFT fft_;
   cudaStream_t stream_ = nullptr;
   Stats stats_;
