@@ -441,6 +441,10 @@ class OracleGridder:
         return cfmod.finalise_grid(self.grids, self.grdsf)
 
     def finalise_weights(self):
+        if self.kind == "AWProject":
+            p = self.aw_params
+            return cfmod.aw_finalise_weights(self.cache.cfs, self.sumw, self.os, self.track_per_os,
+                                             self.cache.offsets, p.maxsupport, self.nx, self.ny, self.nx, self.ny)
         tot = self.sumw.sum(axis=0)  # (npol, nchan)
         return np.broadcast_to(tot[None, None], (self.nx, self.ny) + tot.shape).astype(np.float32)
 

@@ -595,3 +595,64 @@ def wstack_initialise_degrid(image, grdsf, screens):
         work = np.conj(sc(s)).astype(np.complex64)
         out.append(fft2d(work, True))
     return out
+
+
+# --------------------------------------------------------------------------
+# AWProject finaliseWeights
+# --------------------------------------------------------------------------
+def fft_pad(a: np.ndarray, nxo: int, nyo: int) -> np.ndarray:
+    """Fourier-domain interpolation of a real plane to (nxo, nyo), values kept:
+    complex copy scaled by the area ratio, forward transform, the spectrum in
+    the centre of a zero grid, backward transform, real part.  Restated from
+    the steps of SynthesisParamsHelper::oversample with norm = true
+    (askap/measurementequation/SynthesisParamsHelper.cc:918-951); the
+    reference calls base-scimath's PaddingUtils::fftPad (un-vendored), whose
+    exact scaling is not pinned."""
+    cnx, cny = a.shape
+    if (cnx, cny) == (nxo, nyo):
+        return a.astype(F32)
+    A = fft2d(a.astype(np.complex64) * F32(float(nxo) * float(nyo) / (float(cnx) * float(cny))), True)
+    B = np.zeros((nxo, nyo), dtype=np.complex64)
+    x0, y0 = (nxo - cnx) // 2, (nyo - cny) // 2
+    B[x0:x0 + cnx, y0:y0 + cny] = A
+    return fft2d(B, False).real.astype(F32)
+
+
+def aw_finalise_weights(cfs, sumw, os_, track_per_os, offsets, maxsupport, nx, ny, onx, ony):
+    """AWProjectVisGridder::finaliseWeights (AWProjectVisGridder.cc:616-766)
+    without the spheroidal taper: for every sum-of-weights row with data, the
+    CF of its first oversampling plane, centred in a min(maxsupport, n) grid,
+    backward-transformed (unnormalised); wt |val|^2 summed per (pol, chan) in
+    row order, then Fourier-padded to the (padded) image and its centre
+    (onx, ony) kept."""
+    nz, npol, nchan = sumw.shape
+    cnx, cny = min(maxsupport, nx), min(maxsupport, ny)
+    ccx, ccy = cnx // 2, cny // 2
+    cout = np.zeros((cnx, cny, npol, nchan), dtype=F32)
+    for iz in range(nz):
+        if not np.any(sumw[iz] > 0):
+            continue
+        plane = iz if track_per_os else os_ * os_ * iz
+        c = cfs[plane]
+        s = (c.shape[0] - 1) // 2
+        ou, ov = offsets[iz] if offsets else (0, 0)
+        buf = np.zeros((cnx, cny), dtype=np.complex64)
+        for iy in range(-s, s + 1):
+            for ix in range(-s, s + 1):
+                xp, yp = ix + ccx + ou, iy + ccy + ov
+                if 0 <= xp < cnx and 0 <= yp < cny:
+                    buf[xp, yp] = c[ix + s, iy + s]
+        val = (fft2d(buf, False) * F32(float(cnx) * float(cny))).astype(np.complex64)
+        vr, vi = val.real.astype(F32), val.imag.astype(F32)
+        r = (vr * vr - vi * (-vi)).astype(F32)
+        for ch in range(nchan):
+            for p in range(npol):
+                wt = float(sumw[iz, p, ch])
+                cout[:, :, p, ch] = (cout[:, :, p, ch].astype(np.float64) + wt * r.astype(np.float64)).astype(F32)
+    out = np.zeros((onx, ony, npol, nchan), dtype=F32)
+    x0, y0 = (nx - onx) // 2, (ny - ony) // 2
+    for ch in range(nchan):
+        for p in range(npol):
+            full = fft_pad(cout[:, :, p, ch], nx, ny)
+            out[:, :, p, ch] = full[x0:x0 + onx, y0:y0 + ony]
+    return out

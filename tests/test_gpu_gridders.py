@@ -198,6 +198,11 @@ def test_awproject_cf_grid_degrid(ygmod, oracle_mod):
         worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
     assert worst < TOL, worst
     _check_grid(og, gg)
+    # finaliseWeights: CF-weighted sum of |IFFT(CF)|^2, Fourier-padded from 256^2 to 512^2
+    wg = gg.finaliseWeights()
+    wc = og.finalise_weights()
+    assert np.max(wc) > 0
+    assert rel_l2(wg, wc) < 1e-4, rel_l2(wg, wc)
 
 
 # ---- error conditions (ASKAPCHECK) ------------------------------------------

@@ -1137,12 +1137,37 @@ void Gridder::finalise_grid(float* out, bool out_on_device) {
 
 void Gridder::finalise_weights(float* out, bool out_on_device) {
   throw_if(!sumw_.p, YG_ERR_STATE, "Sum of weights not yet initialised");
-  throw_if(kind_ == Kind::AWProject, YG_ERR_UNSUPPORTED,
-           "AWProject finaliseWeights (CF-weighted sum) is not provided; use sum_weights()");
   std::vector<double> sw;
   int rows = 0;
   sum_weights(sw, &rows);
   const int onx = (int)std::lround(nx_ / padding_), ony = (int)std::lround(ny_ / padding_);
+  if (kind_ == Kind::AWProject) {
+    throw_if(!cf_built_, YG_ERR_STATE, "AWProject finaliseWeights needs the convolution functions of the gridding");
+    const int np = npol_ * nchan_;
+    std::vector<int> planes;
+    std::vector<int2> offs;
+    std::vector<double> wts;
+    for (int z = 0; z < rows; ++z) {
+      bool data = false;
+      for (int q = 0; q < np; ++q) data = data || sw[z + (size_t)rows * q] > 0.0;
+      if (!data) continue;
+      planes.push_back(track_per_os_ ? z : os_ * os_ * z);
+      offs.push_back(z < (int)cf_.h_offsets.size() ? cf_.h_offsets[z] : make_int2(0, 0));
+      for (int q = 0; q < np; ++q) wts.push_back(sw[z + (size_t)rows * q]);
+    }
+    const int cnx = std::min(maxsupport_, nx_), cny = std::min(maxsupport_, ny_);
+    DevBuf dout;
+    float* dst = out;
+    if (!out_on_device) {
+      cuda_check(dout.ensure((size_t)onx * ony * np * sizeof(float)), "alloc");
+      dst = dout.as<float>();
+    }
+    rc_check(aw_weights_image(cf_.view(), planes, offs, wts, np, cnx, cny, nx_, ny_, onx, ony, dst, stream_),
+             "AWProject weights");
+    if (!out_on_device)
+      cuda_check(cudaMemcpy(out, dst, (size_t)onx * ony * np * sizeof(float), cudaMemcpyDeviceToHost), "weights");
+    return;
+  }
   std::vector<float> h((size_t)onx * ony * npol_ * nchan_);
   for (int c = 0; c < nchan_; ++c)
     for (int p = 0; p < npol_; ++p) {

@@ -180,3 +180,193 @@ int image_to_grids(ImageFFT& f, const float* image, int nx, int ny, int nplanes,
 }
 
 }  // namespace yg
+
+namespace yg {
+
+// ---------------------------------------------------------------------------
+// AWProject finaliseWeights (AWProjectVisGridder.cc:616-766, no spheroidal
+// taper): for every sum-of-weights row with data, the CF of its first
+// oversampling plane centred in a cnx x cny grid and backward-transformed
+// (unnormalised); wt |val|^2 summed per (pol, chan) in row order in FP32 with
+// the product in FP64; then a Fourier-domain interpolation to the padded image
+// and its centre kept.
+// ---------------------------------------------------------------------------
+__global__ void k_aw_embed(CFView cf, const int* __restrict__ planes, const int2* __restrict__ offs, int nb, int cnx,
+                           int cny, float2* __restrict__ buf) {
+  const long long per = (long long)cnx * cny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nb; i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / per);
+    const int x = (int)(i % cnx), y = (int)((i / cnx) % cny);
+    float2 v = make_float2(0.f, 0.f);
+    const int plane = planes[b];
+    if (plane >= 0) {
+      const int w = cf.size[plane], s = (w - 1) / 2;
+      const int ix = x - cnx / 2 - offs[b].x, iy = y - cny / 2 - offs[b].y;
+      if (ix >= -s && ix <= s && iy >= -s && iy <= s) v = cf.data[cf.off[plane] + (ix + s) + (long long)w * (iy + s)];
+    }
+    const float sg = sgn_in(x, y);
+    buf[i] = make_float2(v.x * sg, v.y * sg);
+  }
+}
+
+__global__ void k_aw_accum(const float2* __restrict__ buf, const double* __restrict__ wts, int nb, int cnx, int cny,
+                           int nplanes, float* __restrict__ acc) {
+  const long long per = (long long)cnx * cny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nplanes; i += (long long)gridDim.x * blockDim.x) {
+    const int pc = (int)(i / per);
+    const long long px = i % per;
+    const int x = (int)(px % cnx), y = (int)(px / cnx);
+    const float sg = sgn_out(x, y, cnx, cny);
+    float a = acc[i];
+    for (int b = 0; b < nb; ++b) {
+      const double wt = wts[(size_t)b * nplanes + pc];
+      if (!(wt > 0.0)) continue;
+      const float2 v = buf[(size_t)b * per + px];
+      const float vr = v.x * sg, vi = v.y * sg;
+      const float r = __fsub_rn(__fmul_rn(vr, vr), __fmul_rn(vi, -vi));
+      a = (float)((double)a + wt * (double)r);
+    }
+    acc[i] = a;
+  }
+}
+
+__global__ void k_real_to_c_scaled(const float* __restrict__ a, float2* __restrict__ out, int nx, int ny, long long total,
+                                   float scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny);
+    out[i] = make_float2(__fmul_rn(a[i], scale) * sgn_in(x, y), 0.f);
+  }
+}
+
+// spectrum (centred, cnx x cny, forward-transformed with the checkerboard)
+// into the centre of an nx x ny zero grid, ready for the backward transform
+__global__ void k_embed_spectrum(const float2* __restrict__ in, int cnx, int cny, float2* __restrict__ out, int nx,
+                                 int ny, long long total) {
+  const int x0 = (nx - cnx) / 2, y0 = (ny - cny) / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny);
+    const long long p = i / ((long long)nx * ny);
+    const int cx = x - x0, cy = y - y0;
+    float2 v = make_float2(0.f, 0.f);
+    if (cx >= 0 && cy >= 0 && cx < cnx && cy < cny) {
+      v = in[(size_t)p * cnx * cny + cx + (size_t)cnx * cy];
+      const float so = sgn_out(cx, cy, cnx, cny);
+      v.x *= so;
+      v.y *= so;
+    }
+    const float si = sgn_in(x, y);
+    out[i] = make_float2(v.x * si, v.y * si);
+  }
+}
+
+// out[onx, ony, planes] = centre of real(sgn_out * in) / (nx ny)
+__global__ void k_extract_real(const float2* __restrict__ in, int nx, int ny, float inv_n, float* __restrict__ out,
+                               int onx, int ony, long long total) {
+  const int x0 = (nx - onx) / 2, y0 = (ny - ony) / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int ox = (int)(i % onx), oy = (int)((i / onx) % ony);
+    const long long p = i / ((long long)onx * ony);
+    const int x = ox + x0, y = oy + y0;
+    const float2 v = in[(size_t)p * nx * ny + x + (size_t)nx * y];
+    out[i] = __fmul_rn(v.x * sgn_out(x, y, nx, ny), inv_n);
+  }
+}
+
+__global__ void k_extract_plain(const float* __restrict__ in, int nx, int ny, float* __restrict__ out, int onx, int ony,
+                                long long total) {
+  const int x0 = (nx - onx) / 2, y0 = (ny - ony) / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int ox = (int)(i % onx), oy = (int)((i / onx) % ony);
+    const long long p = i / ((long long)onx * ony);
+    out[i] = in[(size_t)p * nx * ny + (ox + x0) + (size_t)nx * (oy + y0)];
+  }
+}
+
+int aw_weights_image(const CFView& cf, const std::vector<int>& planes, const std::vector<int2>& offs,
+                     const std::vector<double>& wts, int nplanes, int cnx, int cny, int nx, int ny, int onx, int ony,
+                     float* out, cudaStream_t st) {
+  const int nrows = (int)planes.size();
+  const long long per = (long long)cnx * cny;
+  DevBuf acc;
+  IM_TRY(acc.ensure((size_t)per * nplanes * sizeof(float)));
+  IM_TRY(cudaMemsetAsync(acc.p, 0, (size_t)per * nplanes * sizeof(float), st));
+  if (nrows > 0) {
+    const int B = std::min(nrows, 32);
+    DevBuf buf, dplanes, doffs, dwts;
+    IM_TRY(buf.ensure((size_t)per * B * sizeof(float2)));
+    IM_TRY(dplanes.ensure(B * sizeof(int)));
+    IM_TRY(doffs.ensure(B * sizeof(int2)));
+    IM_TRY(dwts.ensure((size_t)B * nplanes * sizeof(double)));
+    cufftHandle plan;
+    int dims[2] = {cny, cnx};
+    if (cufftPlanMany(&plan, 2, dims, nullptr, 1, cnx * cny, nullptr, 1, cnx * cny, CUFFT_C2C, B) != CUFFT_SUCCESS)
+      return YG_ERR_CUDA;
+    cufftSetStream(plan, st);
+    int rc = YG_OK;
+    for (int b0 = 0; b0 < nrows && rc == YG_OK; b0 += B) {
+      const int nb = std::min(B, nrows - b0);
+      std::vector<int> pl(B, -1);
+      std::vector<int2> of(B, make_int2(0, 0));
+      std::vector<double> w((size_t)B * nplanes, 0.0);
+      for (int b = 0; b < nb; ++b) {
+        pl[b] = planes[b0 + b];
+        of[b] = offs[b0 + b];
+        for (int q = 0; q < nplanes; ++q) w[(size_t)b * nplanes + q] = wts[(size_t)(b0 + b) * nplanes + q];
+      }
+      if (cudaMemcpyAsync(dplanes.p, pl.data(), B * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(doffs.p, of.data(), B * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+          cudaMemcpyAsync(dwts.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        rc = YG_ERR_CUDA;
+        break;
+      }
+      k_aw_embed<<<blocks_for(per * B), 256, 0, st>>>(cf, dplanes.as<int>(), doffs.as<int2>(), B, cnx, cny,
+                                                      buf.as<float2>());
+      if (cufftExecC2C(plan, (cufftComplex*)buf.p, (cufftComplex*)buf.p, CUFFT_INVERSE) != CUFFT_SUCCESS) {
+        rc = YG_ERR_CUDA;
+        break;
+      }
+      k_aw_accum<<<blocks_for(per * nplanes), 256, 0, st>>>(buf.as<float2>(), dwts.as<double>(), B, cnx, cny, nplanes,
+                                                           acc.as<float>());
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = YG_ERR_CUDA;   // host staging vectors are reused
+    }
+    cufftDestroy(plan);
+    if (rc) return rc;
+  }
+  const long long total_out = (long long)onx * ony * nplanes;
+  if (cnx == nx && cny == ny) {
+    k_extract_plain<<<blocks_for(total_out), 256, 0, st>>>(acc.as<float>(), nx, ny, out, onx, ony, total_out);
+  } else {
+    DevBuf c1, c2;
+    IM_TRY(c1.ensure((size_t)per * nplanes * sizeof(float2)));
+    IM_TRY(c2.ensure((size_t)nx * ny * nplanes * sizeof(float2)));
+    k_real_to_c_scaled<<<blocks_for(per * nplanes), 256, 0, st>>>(
+        acc.as<float>(), c1.as<float2>(), cnx, cny, per * nplanes, (float)((double)nx * ny / ((double)cnx * cny)));
+    cufftHandle p1, p2;
+    int d1[2] = {cny, cnx}, d2[2] = {ny, nx};
+    if (cufftPlanMany(&p1, 2, d1, nullptr, 1, cnx * cny, nullptr, 1, cnx * cny, CUFFT_C2C, nplanes) != CUFFT_SUCCESS)
+      return YG_ERR_CUDA;
+    if (cufftPlanMany(&p2, 2, d2, nullptr, 1, nx * ny, nullptr, 1, nx * ny, CUFFT_C2C, nplanes) != CUFFT_SUCCESS) {
+      cufftDestroy(p1);
+      return YG_ERR_CUDA;
+    }
+    cufftSetStream(p1, st);
+    cufftSetStream(p2, st);
+    int rc = YG_OK;
+    if (cufftExecC2C(p1, (cufftComplex*)c1.p, (cufftComplex*)c1.p, CUFFT_FORWARD) != CUFFT_SUCCESS) rc = YG_ERR_CUDA;
+    const long long tot2 = (long long)nx * ny * nplanes;
+    if (!rc) k_embed_spectrum<<<blocks_for(tot2), 256, 0, st>>>(c1.as<float2>(), cnx, cny, c2.as<float2>(), nx, ny, tot2);
+    if (!rc && cufftExecC2C(p2, (cufftComplex*)c2.p, (cufftComplex*)c2.p, CUFFT_INVERSE) != CUFFT_SUCCESS) rc = YG_ERR_CUDA;
+    if (!rc)
+      k_extract_real<<<blocks_for(total_out), 256, 0, st>>>(c2.as<float2>(), nx, ny,
+                                                           (float)(1.0 / ((double)nx * ny)), out, onx, ony, total_out);
+    cudaStreamSynchronize(st);
+    cufftDestroy(p1);
+    cufftDestroy(p2);
+    if (rc) return rc;
+  }
+  IM_TRY(cudaGetLastError());
+  IM_TRY(cudaStreamSynchronize(st));
+  return YG_OK;
+}
+
+}  // namespace yg

@@ -32,4 +32,11 @@ int image_to_grids(ImageFFT& f, const float* image, int nx, int ny, int nplanes,
                    const std::vector<StackScreen>* screens, int ngrids, const double* corr_x, const double* corr_y,
                    float* corrected_tmp, float2* grids, cudaStream_t st);
 
+// AWProject finaliseWeights: planes[r] = CF index of sum-of-weights row r with
+// data, offs[r] its CF offset, wts[r * nplanes + pol + npol * chan] its
+// weights; out is (onx, ony, nplanes) on the device
+int aw_weights_image(const CFView& cf, const std::vector<int>& planes, const std::vector<int2>& offs,
+                     const std::vector<double>& wts, int nplanes, int cnx, int cny, int nx, int ny, int onx, int ony,
+                     float* out, cudaStream_t st);
+
 }  // namespace yg
