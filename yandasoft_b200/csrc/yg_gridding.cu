@@ -324,7 +324,7 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
                                             const float2* __restrict__ cfpad, int Wp2, int cfbuf, int SB, int NST,
                                             unsigned char* ring, unsigned long long* full,
                                             unsigned long long* empty, int& seg, bool stage_cf = true,
-                                            const float4* __restrict__ ext = nullptr) {
+                                            const float4* __restrict__ ext = nullptr, int nterm = 1) {
   const int lane = threadIdx.x & 31;
   const unsigned fm = 0xffffffffu;
   const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
@@ -394,13 +394,17 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
 #pragma unroll
     for (int p = 0; p < NV; ++p) v[p] = vn[p];
   }
-  const int stage = seg % NST;
-  if (!acquire(stage)) return false;
-  if (lane == 0) {
-    reinterpret_cast<int*>(ring + (size_t)stage * SB + SB - 16)[0] = -1;
-    mbar_arrive(&full[stage]);
+  // end of the item: one terminal segment per consumer that walks its own
+  // subsequence of segments (nterm consecutive ones reach every such walk)
+  for (int q = 0; q < nterm; ++q) {
+    const int stage = seg % NST;
+    if (!acquire(stage)) return false;
+    if (lane == 0) {
+      reinterpret_cast<int*>(ring + (size_t)stage * SB + SB - 16)[0] = -1;
+      mbar_arrive(&full[stage]);
+    }
+    ++seg;
   }
-  ++seg;
   return true;
 }
 
@@ -1017,6 +1021,7 @@ struct DegridTArgs {
   long long ntiles;
   int smax, Pg, Wp, cfbuf;
   int stage_bytes, nstages;
+  int own;                   // segments owned by one warp each (needs nstages >= tap warps)
   LearnedCF lcf;             // the network of the learned CF mode
   const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   float2* out;
@@ -1029,8 +1034,16 @@ struct DegridTArgs {
 //
 // CFM 3: the continuous learned CF, every lane evaluating the network for its
 // taps of every sample at the sample's exact offsets and w.
+//
+// With a.own (not in CFM 2, whose planes the warps evaluate together, and only
+// with at least one stage per tap warp), segment s belongs to tap warp
+// s mod ncw, which alone waits for it, degrids all its samples and releases
+// its stage (empty barriers of count 1): warps do not touch the barriers of
+// segments that are not theirs.  Otherwise every warp walks every segment and
+// takes the samples whose index in the item is its own modulo ncw.
 template <int NPOL, int CFM>
 __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
+  const bool OWN = CFM != 2 && a.own;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int Pg = a.Pg, PG2 = Pg * Pg;
   const int Wp = a.Wp, Wp2 = Wp * Wp;
@@ -1061,7 +1074,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
     s_abort = 0;
     for (int q = 0; q < NST; ++q) {
       mbar_init(&full[q], 1);
-      mbar_init(&empty[q], ncw);
+      mbar_init(&empty[q], OWN ? 1 : ncw);
     }
     mbar_fence_init();
   }
@@ -1077,7 +1090,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   int nfill = 0;
   if (warp == ncw) {
     if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill,
-                        CFM == 0, CFM == 3 ? a.ext : nullptr)) {
+                        CFM == 0, CFM == 3 ? a.ext : nullptr, OWN ? ncw : 1)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -1089,7 +1102,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
     const int steps = Wp2 / 32;        // Wp is a multiple of 16: Wp^2 / 32 is a multiple of 8
     const int rows_per_step = 32 / Wp; // 2 when Wp == 16, else 0 (wrap handled below)
     int cur_cfi = -1;
-    for (int nseg = 0;; ++nseg) {
+    for (int nseg = OWN ? warp : 0;; nseg += OWN ? ncw : 1) {
       const int stage = nseg % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
@@ -1108,7 +1121,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
         const int4 r0 = recs[0];
         learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, 32 * ncw, cur_cfi);
       }
-      for (int l = CFM == 2 ? warp : (warp - g0 % ncw + ncw) % ncw; l < cnt; l += ncw) {
+      for (int l = OWN ? 0 : (CFM == 2 ? warp : (warp - g0 % ncw + ncw) % ncw); l < cnt; l += OWN ? 1 : ncw) {
         const int4 r = recs[l];
         float4 xe = make_float4(0.f, 0.f, 0.f, 0.f);
         if (CFM == 3) xe = xs[l];
@@ -1195,16 +1208,16 @@ size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf, int nst) {
   return degrid_t_tile_bytes(npol, Pg) + (size_t)nst * (seg_stage_bytes(cfbuf, 0) + 16);
 }
 
-// Ring depth of k_degrid_t: up to 12 stages (a few more than the tap warps,
-// which work on different segments), as many as fit with two CTAs per SM when
-// at least min_stages_two_ctas do, else as many as fit one CTA; 0 when not
-// even 2 fit.
+// Ring depth of k_degrid_t: up to 16 stages (two per tap warp, each warp
+// owning every eighth segment), as many as fit with two CTAs per SM when at
+// least min_stages_two_ctas do, else as many as fit one CTA; 0 when not even 2
+// fit.
 int degrid_t_stages(int npol, int Pg, int cfbuf) {
   const size_t tile = degrid_t_tile_bytes(npol, Pg);
   const size_t stage = (size_t)seg_stage_bytes(cfbuf, 0) + 16;
   if (tile + min_stages_two_ctas(stage) * stage <= 113 * 1024)
-    return (int)std::min<size_t>(12, (113 * 1024 - tile) / stage);
-  if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(12, (227 * 1024 - tile) / stage);
+    return (int)std::min<size_t>(16, (113 * 1024 - tile) / stage);
+  if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(16, (227 * 1024 - tile) / stage);
   return 0;
 }
 
@@ -1801,6 +1814,7 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
       smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
     }
     d.stage_bytes = seg_stage_bytes(d.cfbuf, xv);
+    d.own = d.nstages >= kDegridThreads / 32 ? 1 : 0;
     if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
       const int threads = kDegridThreads + 32;   // tap warps + the producer warp
