@@ -238,6 +238,8 @@ struct GridKArgs {
   int npol_total;            // polarisations of the visibility cube
   int stage_bytes;           // bytes of one segment stage
   int nstages;               // depth of the segment ring
+  int pps;                   // CF planes (runs) per stage, CFM 0
+  int cfplane;               // bytes of one CF plane slot
   LearnedCF lcf;             // the network of the learned CF mode
   const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   DevError* err;
@@ -324,7 +326,8 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
                                             const float2* __restrict__ cfpad, int Wp2, int cfbuf, int SB, int NST,
                                             unsigned char* ring, unsigned long long* full,
                                             unsigned long long* empty, int& seg, bool stage_cf = true,
-                                            const float4* __restrict__ ext = nullptr, int nterm = 1) {
+                                            const float4* __restrict__ ext = nullptr, int nterm = 1, int pps = 1,
+                                            int cfplane = 0) {
   const int lane = threadIdx.x & 31;
   const unsigned fm = 0xffffffffu;
   const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
@@ -358,34 +361,51 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
     const int zprev = __shfl_up_sync(fm, r.z, 1);
     unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || zprev != r.z));
     while (heads) {
+      // a stage takes up to pps consecutive runs of the window, each CF plane
+      // in a slot of its own; with pps > 1 the staged records carry the slot
+      // in place of the CF index
       const int h = __ffs(heads) - 1;
-      heads &= heads - 1;
-      const int h2 = heads ? __ffs(heads) - 1 : nwin;
+      unsigned rest = heads & (heads - 1);
+      int nr = 1;
+      while (nr < pps && rest) {
+        rest &= rest - 1;
+        ++nr;
+      }
+      const int h2 = rest ? __ffs(rest) - 1 : nwin;
+      const unsigned grp = heads & ~rest;
+      heads = rest;
       const int stage = seg % NST;
       if (!acquire(stage)) return false;
       unsigned char* sp = ring + (size_t)stage * SB;
       if (lane >= h && lane < h2) {
-        reinterpret_cast<int4*>(sp + cfbuf)[lane - h] = r;
+        int4 rr = r;
+        if (pps > 1) rr.z = __popc(grp & (0xffffffffu >> (31 - lane))) - 1;
+        reinterpret_cast<int4*>(sp + cfbuf)[lane - h] = rr;
         float2* vs = reinterpret_cast<float2*>(sp + cfbuf + kSeg * 16);
 #pragma unroll
         for (int p = 0; p < NV; ++p) vs[(lane - h) * NV + p] = v[p];
         if (ext) reinterpret_cast<float4*>(sp + cfbuf + kSeg * 16 + kSeg * NV * 8)[lane - h] = x;
       }
-      const int cfi = __shfl_sync(fm, r.z, h);
       if (lane == 0) {
         int* hdr = reinterpret_cast<int*>(sp + SB - 16);
         hdr[0] = h2 - h;
         hdr[1] = base + h - it.y;
       }
       __syncwarp();
-      if (lane == 0) {
-        if (stage_cf) {
+      if (stage_cf) {
+        if (lane == 0) {
           fence_proxy_async_smem();
-          mbar_expect_tx(&full[stage], cfcopy);
-          bulk_g2s(sp, cfpad + (size_t)cfi * Wp2, cfcopy, &full[stage]);
-        } else {
-          mbar_arrive(&full[stage]);
+          mbar_expect_tx(&full[stage], (unsigned)nr * cfcopy);
         }
+        unsigned g = grp;
+        for (int k = 0; k < nr; ++k) {
+          const int hk = __ffs(g) - 1;
+          g &= g - 1;
+          const int cfi = __shfl_sync(fm, r.z, hk);
+          if (lane == 0) bulk_g2s(sp + (size_t)k * cfplane, cfpad + (size_t)cfi * Wp2, cfcopy, &full[stage]);
+        }
+      } else if (lane == 0) {
+        mbar_arrive(&full[stage]);
       }
       ++seg;
     }
@@ -514,7 +534,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
   int nfill = 0;       // producer: stages filled
   if (warp == ncw) {
     if (!seg_produce<NPOL>(it, a.rec, a.svis, a.npol_total, a.pol0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full,
-                           empty, nfill, CFS, CFM == 3 ? a.ext : nullptr)) {
+                           empty, nfill, CFS, CFM == 3 ? a.ext : nullptr, 1, CFS ? a.pps : 1, a.cfplane)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -564,7 +584,9 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
       }
       for (int l = 0; l < cnt; ++l) {
         const int4 r = recs[l];
-        const float2* __restrict__ cf_s = CFM == 0 ? cf_stage : (CFM == 1 ? a.cf.pad + (size_t)r.z * Wp2 : plane);
+        const float2* __restrict__ cf_s =
+            CFM == 0 ? (a.pps > 1 ? cf_stage + (size_t)r.z * (a.cfplane / sizeof(float2)) : cf_stage)
+                     : (CFM == 1 ? a.cf.pad + (size_t)r.z * Wp2 : plane);
         float4 xe = make_float4(0.f, 0.f, 0.f, 0.f);
         if (CFM == 3) xe = xs[l];
         const int wcf = (r.y >> 20) & 0x7ff;
@@ -1606,7 +1628,7 @@ int grid_stages(int npol, int Pg, int cfbuf, int nthr) {
 // SM, else for 3 stages with one CTA per SM, for the polarisations of one pass.
 int grid_tile_for(int smax, int npol, bool varsup) {
   const int wpad = ((2 * smax + 1) + 15) / 16 * 16;
-  const int cfbuf = grid_cf_buffer_bytes(wpad);
+  const int cfbuf = (wpad <= 16 ? 4 : 1) * grid_cf_buffer_bytes(wpad);   // the stage's CF slots (see plan_grid)
   const GridShape sh = grid_shape(wpad);
   if (sh.threads == 0) return 16;
   const size_t budgets[2] = {113 * 1024, 227 * 1024};
@@ -1675,7 +1697,10 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.P = P;
   g.Pg = Pg;
   g.Wp = cf.wpad;
-  g.cfbuf = grid_cf_buffer_bytes(cf.wpad);
+  g.cfplane = grid_cf_buffer_bytes(cf.wpad);
+  // small planes come with short runs: several runs share a stage
+  g.pps = (!learned && cf.wpad <= 16) ? 4 : 1;
+  g.cfbuf = g.pps * g.cfplane;
   g.scratch = scratch.as<float2>();
   g.npol_total = v.npol;
   g.err = err;
