@@ -760,6 +760,10 @@ void Gridder::fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, c
   a.cf = cf_.view();
   const int smax = (a.cf.maxsize - 1) / 2;
   a.tile = tile_for(smax, dc.npol);
+  // 16-wide CFs grid with residue rows modulo their real width (exact rows)
+  // unless a layout of several slots per thread was asked for
+  const int wpad16 = ((2 * smax + 1) + 15) / 16 * 16;
+  a.wy = (wpad16 == 16 && grid_variant() <= 1 && exact_rows_) ? 2 * smax + 1 : 0;
   a.ntx = (nx_ + a.tile - 1) / a.tile;
   a.nty = (ny_ + a.tile - 1) / a.tile;
   int mb = 0;

@@ -230,6 +230,7 @@ class Gridder {
   int tile_override_ = 0;
   int vmax_ = 0;   // samples per work item, 0 = automatic
   int grid_mode_ = 0;  // k_grid accumulation variant, 0 = automatic
+  bool exact_rows_ = true;  // 16-wide CFs: residue rows modulo the real CF width
 
   CFCacheDev cf_;
   bool cf_built_ = false;

@@ -240,6 +240,7 @@ struct GridKArgs {
   int nstages;               // depth of the segment ring
   int pps;                   // CF planes (runs) per stage, CFM 0
   int cfplane;               // bytes of one CF plane slot
+  int Wy;                    // row modulus of the residues (the plan's)
   LearnedCF lcf;             // the network of the learned CF mode
   const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   DevError* err;
@@ -561,7 +562,11 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         rowoff[q] = live[q] ? k / Wp : 0;   // ry
       }
     }
-    const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wp;
+    // rows of residues: modulo Wy, the plan's row modulus (the CFs' real width
+    // in the exact-rows layout of 16-wide CFs, one slot per thread; Wp otherwise)
+    const int Wy = a.Wy;
+    const bool rowlive = !RSTEP || rowoff[0] < Wy;
+    const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wy;
     const int trash = Pg * Pg + threadIdx.x;     // target of slots beyond Wp^2
     int cur_cfi = -1;
     for (int nseg_done = 0;; ++nseg_done) {
@@ -596,14 +601,14 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
         const int cb = px0 + Pg * py0;
         const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
-        if (RSTEP) {
+        if (RSTEP && rowlive) {
           int jx = rx[0] - mx;
           jx += (jx < 0) ? Wp : 0;
           int jy0 = rowoff[0] - my;
-          jy0 += (jy0 < 0) ? Wp : 0;
+          jy0 += (jy0 < 0) ? Wy : 0;
           int cell = cb + jx + Pg * jy0;
           int tap = jx + Wp * jy0;
-          const int lim = Wp - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
+          const int lim = Wy - jy0;     // slots with RSTEP*q >= lim wrap to the top rows
           // taps of the padding hold zeros and are accumulated like the others:
           // predicating them off costs more than it saves.  The network is
           // evaluated only inside the CF width.
@@ -611,10 +616,10 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
           for (int q = 0; q < MAXSLOTS; ++q) {
             const bool wrap = RSTEP * q >= lim;
             const int c2 = wrap ? cell - PgW : cell;
-            const int t2 = wrap ? tap - Wp2 : tap;
+            const int t2 = wrap ? tap - Wp * Wy : tap;
             float2 c;
             if (CFM == 3) {
-              const int row = wrap ? jy0 + RSTEP * q - Wp : jy0 + RSTEP * q;
+              const int row = wrap ? jy0 + RSTEP * q - Wy : jy0 + RSTEP * q;
               c = (jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe) : make_float2(0.f, 0.f);
             } else {
               c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
@@ -629,7 +634,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             cell += PgR;
             tap += WpR;
           }
-        } else {
+        } else if (!RSTEP) {
 #pragma unroll
           for (int q = 0; q < MAXSLOTS; ++q) {
             int jx = rx[q] - mx;
@@ -672,7 +677,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
 // padded tile, its residues mod W and the CF width, the CF index, the sample id.
 __global__ void k_records(const unsigned int* __restrict__ val, const unsigned int* __restrict__ pos,
                           const int* __restrict__ cfi, const unsigned long long* __restrict__ key, long long nvalid,
-                          int mbits, int ncf, long long ntiles, int ntx, int tile, int smax, int Wp,
+                          int mbits, int ncf, long long ntiles, int ntx, int tile, int smax, int Wp, int Wy,
                           const int* __restrict__ cfsize, int4* __restrict__ rec) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
     const unsigned int s = val[i];
@@ -684,7 +689,7 @@ __global__ void k_records(const unsigned int* __restrict__ val, const unsigned i
     const int tx = (int)(t % ntx), ty = (int)(t / ntx);
     const int px0 = (int)(ps & 0xffffu) - sup - (tx * tile - smax);
     const int py0 = (int)(ps >> 16) - sup - (ty * tile - smax);
-    rec[i] = make_int4(px0 | (py0 << 16), (px0 % Wp) | ((py0 % Wp) << 10) | (w << 20), c, (int)s);
+    rec[i] = make_int4(px0 | (py0 << 16), (px0 % Wp) | ((py0 % Wy) << 10) | (w << 20), c, (int)s);
   }
 }
 
@@ -1338,6 +1343,7 @@ static int ceil_log2(unsigned long long v) {
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st) {
   const long long n = a.nrow * (long long)a.nchan;
   pl.nsamples = n;
+  pl.wy = a.wy > 0 ? a.wy : a.cf.wpad;
   pl.prev_ready = false;
   pl.ext_ready = false;
   pl.mbits = a.mbits;
@@ -1443,7 +1449,7 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     k_records<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.val.as<unsigned int>(), pl.pos.as<unsigned int>(),
                                                         pl.cfi.as<int>(), pl.key.as<unsigned long long>(), pl.nvalid,
                                                         a.mbits, a.cf.ncf, (long long)a.ntx * a.nty, a.ntx, a.tile,
-                                                        pl.smax, a.cf.wpad, a.cf.size, pl.rec.as<int4>());
+                                                        pl.smax, a.cf.wpad, pl.wy, a.cf.size, pl.rec.as<int4>());
     YG_COUNT_LAUNCH();
   }
   YG_CUDA_TRY(cudaGetLastError());
@@ -1672,7 +1678,12 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
   const int P = pl.pad;
   const int Pg = grid_tile_stride(pl.tile, cf.wpad, pl.smax, cf.varsup != 0);
-  const GridShape shape = learned ? grid_shape_learned(cf.wpad) : grid_shape_variant(cf.wpad, mode);
+  GridShape shape = learned ? grid_shape_learned(cf.wpad) : grid_shape_variant(cf.wpad, mode);
+  if (pl.wy != cf.wpad) {
+    // exact rows: thread t owns x residue t mod 16 and y residue t / 16 < wy
+    if (cf.wpad != 16 || pl.wy > 16 || (!learned && mode > 1)) return YG_ERR_UNSUPPORTED;
+    shape = GridShape{(16 * pl.wy + 31) / 32 * 32, 1, 16};
+  }
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
   const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
@@ -1681,6 +1692,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>(), sw, err);
   YG_COUNT_LAUNCH();
   GridKArgs g;
+  g.Wy = pl.wy;
   g.items = pl.items.as<int4>();
   g.val = pl.val.as<unsigned int>();
   g.rec = pl.rec.as<int4>();

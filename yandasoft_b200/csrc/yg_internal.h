@@ -83,6 +83,7 @@ struct BinArgs {
   int tile;                // tile side T
   int ntx, nty;            // tiles per axis
   int mbits;               // bits of the within-tile Morton code
+  int wy;                  // row modulus of the residues in the records (0: the padded CF width)
   unsigned long long invalid_key;  // one past the largest valid key
   CFView cf;
 };
@@ -111,6 +112,7 @@ struct Plan {
   DevBuf ext;                   // continuous learned CF: per sorted sample (ru, rv, w, 0)
   bool ext_ready = false;
   int mbits = 0, ncf = 0;       // sort-key layout
+  int wy = 0;                   // row modulus of the records' residues
   double taps = 0;              // sum of (2S+1)^2 over valid samples (per pol)
 };
 
