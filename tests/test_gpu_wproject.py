@@ -159,3 +159,42 @@ def test_grid_linearity_and_plan_reuse(wp):
         gx.grid(Accessor(ds.uvw, ds.freq, v, noise=ds.noise, flag=ds.flag))
         res.append(gx.grids()[0])
     assert rel_l2(res[2], a * res[0] + b * res[1]) < 1e-5
+
+
+def test_clone_carries_last_visibility(ygmod, oracle_mod):
+    """A clone made after gridding starts from the visibility its prototype
+    last carried (the copy constructor copies itsImagePolFrameVis,
+    TableVisGridder.cc:156): off-grid samples that the clone degrids before
+    its first on-grid one receive that value, as in the reference.  A 512^2
+    grid at 30" keeps most long baselines off the grid and the first rows
+    off-grid."""
+    import math
+
+    import oracle
+    from yandasoft_b200 import simulate
+    from yandasoft_b200.gridder import Accessor, Axes, VisGridderFactory
+    ds = simulate.make_dataset(duration_s=120.0, nchan=2, seed=11)
+    nx, cell = 512, 30.0 * ARCSEC
+    wmax = float(np.max(np.abs(ds.uvw[:, 2])) * ds.freq.max() / simulate.C_LIGHT) * 1.05
+    g = VisGridderFactory.make({"gridder": "WProject", "gridder.WProject.wmax": wmax,
+                                "gridder.WProject.nwplanes": 9, "gridder.WProject.oversample": 4,
+                                "gridder.WProject.maxsupport": 256})
+    g.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    g.grid(Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag))
+    og = oracle.OracleGridder("WProject", wmax=wmax, nwplanes=9, oversample=4, maxsupport=256)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag))
+    img = np.zeros((nx, nx, 1, 1), dtype=np.float32, order="F")
+    img[nx // 2 + 3, nx // 2 - 5, 0, 0] = 1.0
+    gd = g.clone()
+    gd.initialiseDegrid(Axes(cell, cell), img)
+    vg = np.zeros_like(ds.vis)
+    gd.degrid(Accessor(ds.uvw, ds.freq, vg))
+    og.initialise_degrid(img, cell, cell)
+    vc = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc))
+    iu, iv, _, _ = oracle.indices(ds.uvw, ds.freq, og.uvcell[0], og.uvcell[1], og.os, nx, nx)
+    s = og.cache.support
+    on = (iu - s > 0) & (iv - s > 0) & (iu + s < nx) & (iv + s < nx)
+    assert not on[0, 0]
+    assert rel_l2(vg, vc) < TOL, rel_l2(vg, vc)

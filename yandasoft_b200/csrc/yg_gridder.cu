@@ -380,6 +380,14 @@ std::unique_ptr<Gridder> Gridder::clone() const {
     g->learn_wnorm_ = learn_wnorm_;
     g->cf_form_ = cf_form_;
   }
+  if (device_ready_) {
+    // the copy constructor copies itsImagePolFrameVis (TableVisGridder.cc:156):
+    // off-grid samples that a clone degrids before its first on-grid one take
+    // the value this gridder last carried
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    g->ensure_device();
+    cuda_check(cudaMemcpy(g->carry_.p, carry_.p, 8 * sizeof(float2), cudaMemcpyDeviceToDevice), "carry copy");
+  }
   return g;
 }
 
