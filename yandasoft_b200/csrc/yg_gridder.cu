@@ -392,12 +392,17 @@ std::unique_ptr<Gridder> Gridder::clone() const {
 }
 
 Gridder::~Gridder() {
-  if (copy_stream_) {
-    cudaStreamSynchronize(copy_stream_);
-    cudaStreamDestroy(copy_stream_);
+  for (cudaStream_t* cs : {&copy_stream_, &down_stream_}) {
+    if (*cs) {
+      cudaStreamSynchronize(*cs);
+      cudaStreamDestroy(*cs);
+    }
   }
   for (auto& e : piece_up_)
     if (e) cudaEventDestroy(e);
+  for (auto& e : piece_down_)
+    if (e) cudaEventDestroy(e);
+  if (piece_done_) cudaEventDestroy(piece_done_);
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
@@ -898,6 +903,8 @@ Chunk Gridder::stage_rows(const Chunk& c, long long r0, long long nr, int b, boo
                "upload rows");
     return d.p;
   };
+  // the buffers' last piece may still be going back to the host
+  if (piece_down_[b]) cuda_check(cudaStreamWaitEvent(cs, piece_down_[b], 0), "wait download");
   Chunk dc = c;
   dc.nrow = nr;
   dc.uvw = (const double*)up(s.uvw, c.uvw + 3 * r0, nrows * 3 * sizeof(double));
@@ -916,6 +923,11 @@ Chunk Gridder::stage_rows(const Chunk& c, long long r0, long long nr, int b, boo
 
 void Gridder::run_pieces(Chunk& c, bool degridding) {
   if (!copy_stream_) cuda_check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "stream");
+  if (degridding && !down_stream_) {
+    cuda_check(cudaStreamCreateWithFlags(&down_stream_, cudaStreamNonBlocking), "stream");
+    cuda_check(cudaEventCreateWithFlags(&piece_done_, cudaEventDisableTiming), "event");
+    for (auto& e : piece_down_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  }
   const double bytes = (double)c.nrow * c.nchan * c.npol * sizeof(float2);
   const int K = (int)std::max(2.0, std::min(16.0, std::ceil(bytes / kPipePieceBytes)));
   const long long rows = (c.nrow + K - 1) / K;
@@ -927,8 +939,8 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
     const long long r0 = k * rows, nr = std::min(rows, c.nrow - r0);
     if (k + 1 < npieces) {
       // buffer b ^ 1 was last used by piece k - 1, which has finished (the
-      // passes below end on a host synchronisation); a degridded piece's
-      // download was queued on the copy stream before this upload
+      // passes below end on a host synchronisation); the upload waits for
+      // that piece's download (stage_rows)
       const long long r1 = (k + 1) * rows;
       staged[b ^ 1] = stage_rows(c, r1, std::min(rows, c.nrow - r1), b ^ 1, true);
     }
@@ -940,15 +952,20 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
     bin(dc, piece_plan_[b]);
     if (degridding) {
       degrid_plan(dc, piece_plan_[b]);
+      // the download runs on a stream of its own, beside the next upload
+      cuda_check(cudaEventRecord(piece_done_, stream_), "event");
+      cuda_check(cudaStreamWaitEvent(down_stream_, piece_done_, 0), "wait degrid");
       cuda_check(cudaMemcpy2DAsync((char*)c.vis + r0 * sizeof(float2), (size_t)c.nrow * sizeof(float2), dc.vis,
                                    (size_t)nr * sizeof(float2), (size_t)nr * sizeof(float2),
-                                   (size_t)c.nchan * c.npol, cudaMemcpyDeviceToHost, copy_stream_),
+                                   (size_t)c.nchan * c.npol, cudaMemcpyDeviceToHost, down_stream_),
                  "download rows");
+      cuda_check(cudaEventRecord(piece_down_[b], down_stream_), "event");
     } else {
       grid_plan(dc, piece_plan_[b]);
     }
   }
   cuda_check(cudaStreamSynchronize(copy_stream_), "pieces");
+  if (degridding) cuda_check(cudaStreamSynchronize(down_stream_), "pieces");
 }
 
 void Gridder::grid(const Chunk& c) {
