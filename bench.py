@@ -13,6 +13,14 @@ Workloads (seeded synthetic data with the shapes of the benchmark configs):
               grid at 4", 17 w-stacks x 33 w-planes, oversample 8.  Default.
   --config 0  WProject: 36 antennas, 1 h at 10 s, 8 channels 940-948 MHz, XX,
               2048^2 at 8", 65 w-planes, oversample 4.
+  --config 2  AWProject, 36 beams: 12 m dishes with 1 m blockage, a 6 x 6 beam
+              footprint at 0.9 deg pitch (beams observed in turn, one 5 s
+              integration each), 2 h at 5 s (1440 integrations), 48 channels
+              700-1000 MHz, 2 polarisations (87,091,200 samples), sources
+              attenuated by each beam's power pattern.  One imaging instance
+              per beam (rows phased to the beam centre, 2048^2 x 2 grid at 4"),
+              33 w-planes, oversample 4, a CF set per channel built on the GPU;
+              all beams' degrid -> subtract -> grid in one CUDA graph.
 
 `value` is measured with inputs resident in HBM (plan-based passes on device
 buffers); `e2e` goes through the C-ABI IVisGridder calls with pinned host
@@ -49,8 +57,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 3],
-                    help="0, 1: one instance; 3: 64 uneven instances, major cycles as one CUDA graph")
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="0, 1: one instance; 2: one instance per beam; 3: 64 uneven instances, major cycles as "
+                         "one CUDA graph")
     ap.add_argument("--instances", type=int, default=64, help="config 3: number of imaging instances")
     ap.add_argument("--cycles", type=int, default=5, help="config 3: major cycles timed")
     ap.add_argument("--no-e2e", action="store_true")
@@ -74,6 +83,11 @@ def workload(cfg: int, scale: float = 1.0):
                     duration=3600.0 * scale, dt=10.0, f0=940e6, f1=948e6, nchan=8, npol=1, nsrc=20, ngauss=0,
                     field=2.0, sigma=0.01, nx=2048, cell=8.0, nwplanes=65, oversample=4, cutoff=1e-3,
                     maxsupport=1024, seed=0)
+    if cfg == 2:
+        return dict(name="config2_awproject_36beams_2048x2pol", gridder="AWProject", nant=36, diameter=6000.0,
+                    lat=-26.7, dec=-45.0, duration=7200.0 * scale, dt=5.0, f0=700e6, f1=1000e6, nchan=48, npol=2,
+                    nsrc=100, ngauss=0, field=2.0, sigma=0.01, nx=2048, cell=4.0, nwplanes=33, oversample=4,
+                    cutoff=1e-3, maxsupport=256, seed=2, nbeam=36, pitch=0.9, dish=12.0, blockage=1.0)
     return dict(name="config1_wstack17_wproject33_4096x4pol", gridder="WStackWProject", nant=36, diameter=6000.0,
                 lat=-26.7, dec=-45.0, duration=8 * 3600.0 * scale, dt=5.0, f0=700e6, f1=1000e6, nchan=96, npol=4,
                 nsrc=200, ngauss=10, field=2.0, sigma=0.01, nx=4096, cell=4.0, nwstacks=17, nwplanes=33, oversample=8,
@@ -101,6 +115,17 @@ def gen_device(w):
         comp[g, 5] = rng.uniform(0, math.pi, len(g))
     dev = torch.device("cuda")
     nrow = uvw.shape[0]
+    feed = att = feed_d = foot = None
+    if w.get("nbeam"):
+        # beams observed in turn, one integration each; each beam's rows are
+        # phased to the beam's centre and every source is attenuated by the
+        # beam's power pattern
+        feed = simulate.multibeam_rows(ntime, nbl, w["nbeam"])
+        pw, foot = beam_power(w, comp, freq)
+        att = torch.from_numpy(pw).to(dev)
+        feed_d = torch.from_numpy(feed).to(dev)
+        lb = torch.from_numpy(np.sin(foot[:, 0]) * np.cos(foot[:, 1])).to(dev)
+        mb = torch.from_numpy(np.sin(foot[:, 1])).to(dev)
     U = torch.from_numpy(uvw).to(dev)
     F = torch.from_numpy(freq).to(dev)
     l = torch.from_numpy(comp[:, 1]).to(dev)
@@ -117,7 +142,14 @@ def gen_device(w):
     for r0 in range(0, nrow, R):
         r1 = min(nrow, r0 + R)
         u, v, ww = U[r0:r1, 0:1], U[r0:r1, 1:2], U[r0:r1, 2:3]
-        cyc = (l[None] * u + m[None] * v + (n[None] - 1) * ww) / C_LIGHT       # cycles per Hz (FP64)
+        if att is None:
+            cyc = (l[None] * u + m[None] * v + (n[None] - 1) * ww) / C_LIGHT       # cycles per Hz (FP64)
+        else:
+            fr = feed_d[r0:r1].long()
+            lr = l[None] - lb[fr][:, None]
+            mr = m[None] - mb[fr][:, None]
+            nr = torch.sqrt(1 - lr * lr - mr * mr)
+            cyc = (lr * u + mr * v + (nr - 1) * ww) / C_LIGHT
         r = None
         if bool(gauss.any()):
             up = (torch.cos(bpa)[None] * u + torch.sin(bpa)[None] * v) / C_LIGHT
@@ -128,6 +160,8 @@ def gen_device(w):
             ph = cyc * f
             ph = (ph - torch.floor(ph)).float() * (2 * math.pi)
             amp = flux[None].expand_as(ph)
+            if att is not None:
+                amp = amp * att[fr, :, c]
             if r is not None:
                 amp = amp * torch.exp(-r * f * f)
             amp = amp.float()
@@ -146,7 +180,7 @@ def gen_device(w):
     del model
     wmax_data = float(torch.max(torch.abs(U[:, 2]))) * float(freq.max()) / C_LIGHT
     return dict(uvw=U, freq=F, vis=vis, nrow=nrow, nchan=nchan, npol=npol, freq_np=freq, uvw_np=uvw, sky=comp,
-                wmax=math.ceil(wmax_data * 1.02 / 100.0) * 100.0)
+                wmax=math.ceil(wmax_data * 1.02 / 100.0) * 100.0, feed_np=feed, foot=foot)
 
 
 def parset_for(w, wmax):
@@ -156,7 +190,35 @@ def parset_for(w, wmax):
          "gridder.%s.maxsupport" % g: w["maxsupport"]}
     if g == "WStackWProject":
         p["gridder.%s.nwstacks" % g] = w["nwstacks"]
+    if g == "AWProject":
+        p["gridder.%s.maxfeeds" % g] = 1          # one beam per imaging instance
+        p["gridder.%s.diameter" % g] = "%gm" % w["dish"]
+        p["gridder.%s.blockage" % g] = "%gm" % w["blockage"]
     return p
+
+
+def beam_power(w, comp, freq):
+    """Power pattern of each beam at each source, (nbeam, nsrc, nchan): the
+    far field of a uniformly illuminated annular aperture (dish diameter D,
+    central blockage d) at the source's distance from the beam centre,
+    V = (D^2 jinc(pi D theta / lambda) - d^2 jinc(pi d theta / lambda)) / (D^2 - d^2)
+    with jinc(x) = 2 J1(x) / x, and P = V^2."""
+    from scipy.special import j1
+    from yandasoft_b200 import simulate
+    foot = simulate.beam_footprint(int(round(math.sqrt(w["nbeam"]))), w["pitch"])
+    lb = np.sin(foot[:, 0]) * np.cos(foot[:, 1])
+    mb = np.sin(foot[:, 1])
+    theta = np.hypot(comp[None, :, 1] - lb[:, None], comp[None, :, 2] - mb[:, None])     # (nbeam, nsrc)
+    lam = C_LIGHT / np.asarray(freq)
+
+    def jinc(x):
+        x = np.where(x == 0, 1e-30, x)
+        return 2.0 * j1(x) / x
+
+    D, b = w["dish"], w["blockage"]
+    x = math.pi * theta[:, :, None] / lam[None, None, :]
+    v = (D * D * jinc(D * x) - b * b * jinc(b * x)) / (D * D - b * b)
+    return (v * v).astype(np.float64), foot
 
 
 def model_image(w, sky, npol):
@@ -306,6 +368,104 @@ def cpu_baseline(w, d, target_s=15.0, threads=None):
                              sample="%d of %d rows (every %d-th), all %d channels x %d pols; one degrid + one grid "
                                     "pass; %d threads over channel slices, each with its own %.1f GB of grids"
                              % (len(rows), nrow_all, step, len(freq), d["npol"], threads, grid_bytes / 1e9))
+
+
+def cpu_baseline_aw(w, d, ps=None, target_s=15.0, threads=None):
+    """AWProject, one beam's imaging instance (the footprint's corner beam,
+    its rows phased to its own centre): the oracle's CF generation (the numpy
+    restatement of AWProjectVisGridder::initConvolutionFunction) timed per
+    (beam, channel) set of w-planes, and one degrid + one grid pass of its C
+    gridder on a bounded sample of that beam's rows at every 12th channel,
+    threads over row slices (one gridder each, sharing the CF cache).  With a
+    parset `ps`, the GPU gridder grids the same sample with it and its CF
+    matrices and grid are compared with the oracle's.
+    Returns (Mvis/s, info)."""
+    import concurrent.futures as cf
+    import oracle
+    threads = threads or (os.cpu_count() or 1)
+    nx = w["nx"]
+    cell = w["cell"] * ARCSEC
+    chans = np.arange(0, d["nchan"], 12)
+    rows_all = np.nonzero(d["feed_np"] == 0)[0]
+    freq = np.ascontiguousarray(d["freq_np"][chans])
+    kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
+              maxsupport=w["maxsupport"], maxfeeds=1, diameter=w["dish"], blockage=w["blockage"])
+    g0 = oracle.OracleGridder("AWProject", **kw)
+    g0.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+    t0 = time.perf_counter()
+    # the CF cache depends on the beam, its pointing and the chunk's frequencies
+    g0.init_cf(oracle.Chunk(uvw=np.zeros((1, 3)), freq=freq, vis=None))
+    t_cf = time.perf_counter() - t0
+    njobs = len(chans)
+    support = g0.cache.support
+    taps = (2 * support + 1) ** 2
+    per_sample = 2 * taps * d["npol"] * 1.5e-9 / max(1, threads)
+    nrows = int(min(len(rows_all), max(2000, target_s / (per_sample * len(chans)))))
+    rows = rows_all[np.linspace(0, len(rows_all) - 1, nrows).astype(np.int64)]
+    uvw = np.ascontiguousarray(d["uvw_np"][rows])
+    vis = d["vis"][:, :, torch_index(rows)][:, torch_index(chans), :].cpu().numpy()      # [pol][chan][row]
+    cube = np.asfortranarray(np.transpose(vis, (2, 1, 0)))
+    chunk = oracle.Chunk(uvw=uvw, freq=freq, vis=cube)
+    check = {}
+    if ps is not None:
+        # the GPU gridder on the same sample: CF matrices and grid against the oracle
+        from yandasoft_b200 import gridder as G
+        gs = G.VisGridderFactory.make(ps)
+        gs.initialiseGrid(G.Axes(cell, cell), (nx, nx, d["npol"], 1))
+        gs.grid(G.Accessor(uvw, freq, cube))
+        cf_err = 0.0
+        ncmp = 0
+        for a, b in zip(g0.cache.cfs, gs.convolution_functions()):
+            if a is None:
+                continue
+            cf_err = max(cf_err, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+            ncmp += 1
+        og = oracle.OracleGridder("AWProject", **kw)
+        og.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+        og.grid(chunk)
+        grid_err = float(np.linalg.norm(gs.grids()[0] - og.grids[0]) / np.linalg.norm(og.grids[0]))
+        check = {"sample_cf_matrices_compared": ncmp, "sample_cf_max_rel_err_vs_oracle": cf_err,
+                 "sample_grid_rel_err_vs_oracle": grid_err, "sample_support_gpu": int(gs.support()[0]),
+                 "sample_support_oracle": int(support)}
+        del gs, og
+    slices = np.array_split(np.arange(len(rows)), threads)
+
+    def work(sl):
+        if len(sl) == 0:
+            return 0
+        sub = oracle.Chunk(uvw=np.ascontiguousarray(uvw[sl]), freq=freq, vis=np.asfortranarray(cube[sl]))
+        out = np.zeros_like(sub.vis)
+        gd = oracle.OracleGridder("AWProject", **kw)
+        gd._init_axes(nx, nx, d["npol"], 1, cell, cell, None)
+        gd.psf = False
+        gd.grids = g0.grids
+        gd.cache, gd._flat, gd.aw_params, gd.aw_nchan = g0.cache, g0._flat, g0.aw_params, g0.aw_nchan
+        gd.sumw = np.zeros((1, d["npol"], 1), order="F")
+        gd._run(oracle.Chunk(uvw=sub.uvw, freq=freq, vis=out), forward=True)
+        gg = oracle.OracleGridder("AWProject", **kw)
+        gg.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+        gg.cache, gg._flat, gg.aw_params, gg.aw_nchan = g0.cache, g0._flat, g0.aw_params, g0.aw_nchan
+        gg.sumw = np.zeros_like(g0.sumw)
+        gg._run(sub, forward=False)
+        return sub.vis.size
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        n = sum(ex.map(work, slices))
+    t = time.perf_counter() - t0
+    info = dict(cores=threads, seconds=t,
+                sample="%d of %d rows (beam 0's instance), channels %s of %d, %d pols; one degrid + one grid pass; "
+                       "%d threads over row slices sharing the oracle's CF cache"
+                % (len(rows), d["nrow"], chans.tolist(), d["nchan"], d["npol"], threads),
+                cf={"cpu_port_s_per_beam_channel": round(t_cf / njobs, 3),
+                    "cpu_port_s_all_%d_beams_x_%d_channels" % (w["nbeam"], d["nchan"]):
+                        round(t_cf / njobs * w["nbeam"] * d["nchan"], 1), **check})
+    return n / t / 1e6, info
+
+
+def torch_index(a):
+    import torch
+    return torch.from_numpy(np.asarray(a, dtype=np.int64)).to("cuda")
 
 
 # --------------------------------------------------------------------------
@@ -639,7 +799,10 @@ def run_reference(args, w):
     times = []
     vals = []
     for s in range(args.warmup + args.steps):
-        v, inf = cpu_baseline(w, d, target_s=8.0)
+        if w["gridder"] == "AWProject":
+            v, inf = cpu_baseline_aw(w, d, target_s=8.0)
+        else:
+            v, inf = cpu_baseline(w, d, target_s=8.0)
         if s >= args.warmup:
             vals.append(v)
             times.append(inf["seconds"])
@@ -733,6 +896,149 @@ def run_batch(args):
     print(json.dumps(line))
 
 
+def run_beams(args, w):
+    """Config 2: one AWProject imaging instance per beam (its rows phased to
+    the beam's centre, image centred there, a CF set per channel), a degridder
+    with the beam's model and a gridder for the residual each, over
+    device-resident chunks; the degrid -> subtract -> grid sequence of all
+    beams recorded as one CUDA graph (yandasoft_b200.gridder.MajorCycle) and
+    replayed.  value = visibility samples degridded and gridded per second
+    over all beams; e2e = the same through the C-ABI calls of each beam with
+    pinned host buffers."""
+    import torch
+    from yandasoft_b200 import build
+    from yandasoft_b200 import gridder as G
+    build.build()
+    G.load()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.perf_counter()
+    d = gen_device(w)
+    t_gen = time.perf_counter() - t0
+    nx, npol, nchan = w["nx"], d["npol"], d["nchan"]
+    cell = w["cell"] * ARCSEC
+    axes = G.Axes(cell, cell)
+    ps = parset_for(w, d["wmax"])
+    nvis = d["nrow"] * nchan * npol
+    foot = d["foot"]
+    beams = []
+    t0 = time.perf_counter()
+    for b in range(w["nbeam"]):
+        rows = np.nonzero(d["feed_np"] == b)[0]
+        ri = torch_index(rows)
+        uvw_b = d["uvw"][ri].contiguous()
+        vis_b = d["vis"][:, :, ri].contiguous()
+        acc = G.Accessor(uvw_b, d["freq"], vis_b, shape=(len(rows), nchan, npol))
+        sky_b = d["sky"].copy()
+        sky_b[:, 1] -= math.sin(foot[b, 0]) * math.cos(foot[b, 1])
+        sky_b[:, 2] -= math.sin(foot[b, 1])
+        gd = G.VisGridderFactory.make(ps)
+        gd.initialiseDegrid(axes, model_image(w, sky_b, npol))
+        gg = G.VisGridderFactory.make(ps)
+        gg.initialiseGrid(axes, (nx, nx, npol, 1))
+        beams.append(dict(rows=rows, uvw=uvw_b, vis=vis_b, acc=acc, gd=gd, gg=gg, sky=sky_b))
+    cyc = G.MajorCycle([x["gd"] for x in beams], [x["gg"] for x in beams], [x["acc"] for x in beams])
+    t_build = time.perf_counter() - t0
+    ms_cf = sum(x["gg"].stats()["ms_cf"] + x["gd"].stats()["ms_cf"] for x in beams)
+    support, os_, ncf = beams[0]["gg"].support()
+    for _ in range(args.warmup):
+        cyc.run(1)
+    with ClockSampler(0) as clk:
+        ms = cyc.run(args.steps)
+    ms_step = ms / args.steps
+    taps = (2 * support + 1) ** 2
+    line = {
+        "metric": METRIC, "cf_form": "plain (tabulated CF)",
+        "value": round(nvis / (ms_step / 1e3) / 1e6, 3), "unit": "Mvis/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; see bench.py workload())",
+        "config": {"workload": w["name"], "gridder": "AWProject", "vis_samples": int(nvis), "rows": int(d["nrow"]),
+                   "channels": nchan, "pols": npol, "beams": w["nbeam"], "grid_per_beam": [nx, nx, npol, 1],
+                   "cell_arcsec": w["cell"], "support": int(support), "taps_per_sample": taps,
+                   "oversample": w["oversample"], "dish_m": w["dish"], "blockage_m": w["blockage"],
+                   "footprint": "6x6 at %g deg" % w["pitch"],
+                   "step": "every beam: degrid model, subtract, grid residual (one CUDA graph, %d nodes)"
+                           % cyc.nodes(),
+                   "l2": "inputs (%.2f GB of visibilities, %.1f GB of CF caches) larger than L2"
+                         % (nvis * 8 / 1e9, 2 * w["nbeam"] * ncf * taps * 8 / 1e9),
+                   "generate_s": round(t_gen, 1), "setup_s": round(t_build, 1)},
+        "cf_cache": {"cf_matrices_per_gridder": int(ncf), "gridders": 2 * w["nbeam"],
+                     "built_on": "GPU (cuFFT + own kernels) when each gridder first sees its chunk",
+                     "gpu_build_s_all_gridders": round(ms_cf / 1e3, 3),
+                     "bytes_per_gridder": int(ncf * taps * 8),
+                     "padded_bytes_per_gridder": int(ncf * ((2 * support + 1 + 15) // 16 * 16) ** 2 * 8)},
+        "binding": {"resource": "shared memory", "note": "k_grid and k_degrid_t, whole step",
+                    "taps_per_s": round(2 * taps * nvis / (ms_step / 1e3), 1)},
+        "clocks": clk.summary(),
+        "gpu_launches": int(cyc.nodes() * args.steps),
+        "gpu_launches_note": "graph nodes (kernels and memsets) x steps",
+    }
+    del cyc
+    for x in beams:
+        del x["gd"], x["gg"], x["acc"]
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if not args.no_e2e:
+        line["e2e"] = e2e_beams(args, w, d, beams, ps, axes)
+    if not args.no_cpu:
+        try:
+            v, inf = cpu_baseline_aw(w, d, ps)
+            line["cf_cache"].update(inf["cf"])
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
+                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2)}
+        except Exception as e:  # the baseline must not hide the GPU result
+            line["cpu_baseline"] = {"value": None, "error": repr(e)}
+    print(json.dumps(line))
+
+
+def e2e_beams(args, w, d, beams, ps, axes):
+    """Every beam through the IVisGridder C-ABI calls with pinned host
+    buffers: initialiseDegrid, degrid (host cube in and out), initialiseGrid,
+    grid (host cube in), finaliseGrid (image to host)."""
+    import torch
+    from yandasoft_b200 import gridder as G
+    nx, npol, nchan = w["nx"], d["npol"], d["nchan"]
+    host = []
+    for x in beams:
+        nr = len(x["rows"])
+        vh = torch.empty(x["vis"].shape, dtype=x["vis"].dtype, pin_memory=True)
+        vh.copy_(x["vis"])
+        mh = torch.zeros(x["vis"].shape, dtype=x["vis"].dtype, pin_memory=True)
+        uh = torch.empty(x["uvw"].shape, dtype=x["uvw"].dtype, pin_memory=True)
+        uh.copy_(x["uvw"])
+        cube = vh.numpy().view(np.complex64).reshape(-1).reshape((nr, nchan, npol), order="F")
+        mcube = mh.numpy().view(np.complex64).reshape(-1).reshape((nr, nchan, npol), order="F")
+        host.append(dict(keep=(vh, mh, uh), acc=G.Accessor(uh.numpy(), d["freq_np"], cube),
+                         accm=G.Accessor(uh.numpy(), d["freq_np"], mcube), img=model_image(w, x["sky"], npol)))
+    out = np.zeros((nx, nx, npol, 1), dtype=np.float32, order="F")
+    # one degridder and one gridder serve every beam in turn: each beam's
+    # chunk has the same frequencies and its beam at the image centre, so the
+    # CF caches built for the first stay valid
+    gd, gg = G.VisGridderFactory.make(ps), G.VisGridderFactory.make(ps)
+
+    def step():
+        for h in host:
+            gd.initialiseDegrid(axes, h["img"])
+            gd.degrid(h["accm"])
+            gg.initialiseGrid(axes, (nx, nx, npol, 1))
+            gg.grid(h["acc"])
+            gg.finaliseGrid(out)
+
+    step()   # warm (CF generation, allocations)
+    torch.cuda.synchronize()
+    k = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    torch.cuda.synchronize()
+    t = (time.perf_counter() - t0) / k
+    nvis = d["nrow"] * nchan * npol
+    h2d = nvis * 8 * 2 + d["nrow"] * 24 * 2 + len(host) * (nchan * 8 * 2 + host[0]["img"].nbytes)
+    d2h = nvis * 8 + len(host) * out.nbytes
+    return {"value": round(nvis / t / 1e6, 3), "unit": "Mvis/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": round(t * 1e3, 2),
+            "path": "per beam: C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers"}
+
+
 def main():
     args = parse()
     if args.config == 3:
@@ -741,6 +1047,8 @@ def main():
     w = workload(args.config, args.scale)
     if args.impl == "reference":
         run_reference(args, w)
+    elif args.config == 2:
+        run_beams(args, w)
     else:
         run_b200(args, w)
 

@@ -205,6 +205,59 @@ def test_awproject_cf_grid_degrid(ygmod, oracle_mod):
     assert rel_l2(wg, wc) < 1e-4, rel_l2(wg, wc)
 
 
+def test_awproject_36_beam_footprint(ygmod, oracle_mod):
+    """The 36-beam AWProject case at reduced size, gridded as one mosaic:
+    12 m dishes with 1 m blockage, a 6 x 6 beam footprint at 0.9 deg pitch
+    (beams observed in turn, one integration each), 4 channels over
+    700-1000 MHz with a CF set per channel, 2 polarisations, 33 w-planes,
+    oversample 4.  Reduced (2 km array, 5 min track, 256^2 grid at 30") so
+    that the oracle's 76,032 CF matrices take seconds.  The first row's beam
+    is the footprint's corner, whose w-plane 0 sets the common support."""
+    import oracle
+    from yandasoft_b200 import simulate
+    from yandasoft_b200.gridder import Accessor, Axes
+    ds = simulate.make_dataset(duration_s=300.0, dt_s=5.0, nchan=4, npol=2, seed=21, freq0=700e6, freq1=1000e6,
+                               diameter_m=2000.0)
+    foot = simulate.beam_footprint(6, 0.9)
+    feed = simulate.multibeam_rows(ds.ntime, ds.nbl, 36)
+    pnt = foot[feed]
+    nx, cell = 256, 30.0 * ARCSEC
+    params = {"wmax": _wmax(ds), "nwplanes": 33, "oversample": 4, "maxsupport": 256, "maxfeeds": 36,
+              "diameter": "12m", "blockage": "1m", "cutoff": 1e-3}
+    og, gg = make_pair("AWProject", params)
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 2, 1))
+    gg.grid(Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    og.initialise_grid(nx, nx, 2, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed,
+                         pointing=pnt))
+    assert gg.support()[0] == og.cache.support
+    cpu = og.cache.cfs
+    gpu = gg.convolution_functions()
+    assert len(cpu) == len(gpu) == 36 * 4 * 33 * 16
+    worst = 0.0
+    for a, b in zip(cpu, gpu):
+        worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+    assert worst < TOL, worst
+    _check_grid(og, gg)
+    # degrid a model of points at the central beams' centres through a clone
+    model = np.zeros((nx, nx, 2, 1), dtype=np.float32, order="F")
+    for k, (dx, dy) in enumerate(foot):
+        x, y = nx // 2 + int(round(dx / cell)), nx // 2 + int(round(dy / cell))
+        if 0 <= x < nx and 0 <= y < nx:
+            model[x, y, :, 0] = 0.1 + 0.01 * k
+    assert np.count_nonzero(model) > 0
+    gd = gg.clone()
+    gd.initialiseDegrid(Axes(cell, cell), model)
+    vg = np.zeros_like(ds.vis)
+    gd.degrid(Accessor(ds.uvw, ds.freq, vg, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    og.initialise_degrid(model, cell, cell)
+    vc = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=ds.noise, flag=ds.flag, feed1=feed,
+                           pointing=pnt))
+    assert np.abs(vc).max() > 0
+    assert rel_l2(vg, vc) < TOL, rel_l2(vg, vc)
+
+
 # ---- error conditions (ASKAPCHECK) ------------------------------------------
 def test_w_out_of_range_raises(ygmod):
     from yandasoft_b200.gridder import Accessor, AskapError, Axes, VisGridderFactory

@@ -180,3 +180,19 @@ def config0(seed: int = 0, predict=None, duration_s: float = 3600.0) -> tuple[Da
     params = dict(gridder="WProject", nx=2048, ny=2048, cell_arcsec=8.0, nwplanes=65, oversample=4,
                   cutoff=1e-3, maxsupport=1024, wmax=math.ceil(wmax_data * 1.02 / 100.0) * 100.0)
     return ds, params
+
+
+def beam_footprint(nside: int = 6, pitch_deg: float = 0.9) -> np.ndarray:
+    """Pointing offsets (ra, dec) in radians of a square nside x nside beam
+    footprint at the given pitch, centred on (0, 0), beams in row-major order."""
+    k = (np.arange(nside) - (nside - 1) / 2.0) * pitch_deg * DEG
+    dx, dy = np.meshgrid(k, k, indexing="xy")
+    return np.stack([dx.ravel(), dy.ravel()], 1)
+
+
+def multibeam_rows(ntime: int, nbl: int, nbeam: int, first_beam: int = 0):
+    """Beam (feed) index per row of a track of ntime integrations x nbl
+    baselines when the beams are observed in turn: integration t belongs to
+    beam (first_beam + t) mod nbeam."""
+    t = np.arange(ntime * nbl) // nbl
+    return ((first_beam + t) % nbeam).astype(np.int32)
