@@ -205,6 +205,40 @@ def test_awproject_cf_grid_degrid(ygmod, oracle_mod):
     assert rel_l2(wg, wc) < 1e-4, rel_l2(wg, wc)
 
 
+# ---- WProject parset variants ---------------------------------------------------
+# (parset keys, oracle keywords, generic keys): non-linear w-sampling
+# (PowerWSampling, GaussianWSampling), per-plane supports with peak offsets,
+# limitsupport, an absolute cutoff and sums of weights per oversampling offset
+_VARIANTS = {
+    "powerlaw": ({"wsampling": "powerlaw", "wsampling.exponent": 0.5}, {"wsampling": "powerlaw", "exponent": 0.5},
+                 None),
+    "gaussian": ({"wsampling": "gaussian", "wsampling.nwplanes50": 4.0},
+                 {"wsampling": "gaussian", "nwplanes50": 4.0}, None),
+    "variable_offset_support": ({"variablesupport": True, "offsetsupport": True}, {}, None),
+    "limitsupport": ({"limitsupport": 8}, {}, None),
+    "cutoff_absolute": ({"cutoff.absolute": True}, {}, None),
+    "oversampleweight": ({}, {}, {"gridder.oversampleweight": True}),
+}
+
+
+@pytest.mark.parametrize("variant", sorted(_VARIANTS))
+def test_wproject_parset_variants(ygmod, oracle_mod, variant):
+    keys, okw, generic = _VARIANTS[variant]
+    ds = _data(duration=300.0, nchan=4)
+    nx, cell = 512, 20.0 * ARCSEC
+    params = {"wmax": _wmax(ds), "nwplanes": 9, "oversample": 4, "maxsupport": 256, "cutoff": 1e-3}
+    params.update(keys)
+    og, gg = _run_pair("WProject", params, ds, nx, cell, 1, generic=generic, oracle_kw=okw)
+    cpu = og.cache.cfs
+    gpu = gg.convolution_functions()
+    assert [c.shape for c in cpu] == [c.shape for c in gpu]
+    worst = max(float(np.max(np.abs(a - b)) / np.max(np.abs(a))) for a, b in zip(cpu, gpu))
+    assert worst < TOL, worst
+    _check_grid(og, gg)
+    model, _ = snapped_model(ds, nx, cell, max_nu=0.5, extra=4)
+    _check_degrid(og, gg, ds, model, cell)
+
+
 def test_awproject_36_beam_footprint(ygmod, oracle_mod):
     """The 36-beam AWProject case at reduced size, gridded as one mosaic:
     12 m dishes with 1 m blockage, a 6 x 6 beam footprint at 0.9 deg pitch
