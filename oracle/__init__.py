@@ -444,7 +444,9 @@ class OracleGridder:
         if self.kind == "AWProject":
             p = self.aw_params
             return cfmod.aw_finalise_weights(self.cache.cfs, self.sumw, self.os, self.track_per_os,
-                                             self.cache.offsets, p.maxsupport, self.nx, self.ny, self.nx, self.ny)
+                                             self.cache.offsets, p.maxsupport, self.nx, self.ny, self.nx, self.ny,
+                                             grdsf=self.grdsf if p.spheroidaltaper else None,
+                                             weights_cutoff=float(self.kw.get("spheroidalweightscutoff", 0.0)))
         tot = self.sumw.sum(axis=0)  # (npol, nchan)
         return np.broadcast_to(tot[None, None], (self.nx, self.ny) + tot.shape).astype(np.float32)
 

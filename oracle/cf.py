@@ -618,16 +618,25 @@ def fft_pad(a: np.ndarray, nxo: int, nyo: int) -> np.ndarray:
     return fft2d(B, False).real.astype(F32)
 
 
-def aw_finalise_weights(cfs, sumw, os_, track_per_os, offsets, maxsupport, nx, ny, onx, ony):
-    """AWProjectVisGridder::finaliseWeights (AWProjectVisGridder.cc:616-766)
-    without the spheroidal taper: for every sum-of-weights row with data, the
-    CF of its first oversampling plane, centred in a min(maxsupport, n) grid,
-    backward-transformed (unnormalised); wt |val|^2 summed per (pol, chan) in
-    row order, then Fourier-padded to the (padded) image and its centre
-    (onx, ony) kept."""
+def aw_finalise_weights(cfs, sumw, os_, track_per_os, offsets, maxsupport, nx, ny, onx, ony, grdsf=None,
+                        weights_cutoff=0.0):
+    """AWProjectVisGridder::finaliseWeights (AWProjectVisGridder.cc:616-766):
+    for every sum-of-weights row with data, the CF of its first oversampling
+    plane, centred in a min(maxsupport, n) grid, backward-transformed
+    (unnormalised); wt |val|^2 summed per (pol, chan) in row order, then
+    Fourier-padded to the (padded) image and its centre (onx, ony) kept.
+    With a spheroidal taper (grdsf given, :641-664, :735-745) the taper
+    grdsf(|i - c| / c), zero at or below weights_cutoff, edge interpolated,
+    is divided out of each transformed CF where it is positive."""
     nz, npol, nchan = sumw.shape
     cnx, cny = min(maxsupport, nx), min(maxsupport, ny)
     ccx, ccy = cnx // 2, cny // 2
+    taper = None
+    if grdsf is not None:
+        def tap(n, c):
+            val = grdsf(np.abs(np.arange(n, dtype=np.float64) - float(c)) / float(c))
+            return interpolate_edge_values(np.where(val > weights_cutoff, val, 0.0))
+        taper = (tap(cnx, ccx)[:, None] * tap(cny, ccy)[None, :]).astype(F32)
     cout = np.zeros((cnx, cny, npol, nchan), dtype=F32)
     for iz in range(nz):
         if not np.any(sumw[iz] > 0):
@@ -644,6 +653,11 @@ def aw_finalise_weights(cfs, sumw, os_, track_per_os, offsets, maxsupport, nx, n
                     buf[xp, yp] = c[ix + s, iy + s]
         val = (fft2d(buf, False) * F32(float(cnx) * float(cny))).astype(np.complex64)
         vr, vi = val.real.astype(F32), val.imag.astype(F32)
+        if taper is not None:
+            pos = taper > 0
+            safe = np.where(pos, taper, F32(1.0))
+            vr = np.where(pos, vr / safe, F32(0.0)).astype(F32)
+            vi = np.where(pos, vi / safe, F32(0.0)).astype(F32)
         r = (vr * vr - vi * (-vi)).astype(F32)
         for ch in range(nchan):
             for p in range(npol):

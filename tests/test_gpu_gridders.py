@@ -205,6 +205,67 @@ def test_awproject_cf_grid_degrid(ygmod, oracle_mod):
     assert rel_l2(wg, wc) < 1e-4, rel_l2(wg, wc)
 
 
+def test_awproject_spheroidal_taper(ygmod, oracle_mod):
+    """AWProject with spheroidaltaper: the anti-aliasing spheroidal multiplies
+    the image-plane screen inside the central qnx x qny region
+    (AWProjectVisGridder.cc:338-354, :405-414), finaliseGrid and
+    initialiseDegrid apply the SphFunc grid correction, and finaliseWeights
+    divides the taper (cut at spheroidalweightscutoff) out of every
+    transformed CF."""
+    import oracle
+    from yandasoft_b200.gridder import Accessor, Axes
+    ds = _data(duration=120.0, nchan=2, seed=9, diameter=2000.0)
+    nrow = ds.nrow
+    feed = (np.arange(nrow) % 2).astype(np.int32)
+    pnt = np.zeros((nrow, 2))
+    pnt[feed == 1, 0] = 0.5 * math.pi / 180
+    nx, cell = 512, 10.0 * ARCSEC
+    params = {"wmax": _wmax(ds), "nwplanes": 5, "oversample": 4, "maxsupport": 256, "maxfeeds": 2,
+              "diameter": "25m", "blockage": "2m", "cutoff": 1e-3, "spheroidaltaper": True,
+              "spheroidalweightscutoff": 1e-3}
+    og, gg = make_pair("AWProject", params, oracle_kw={"spheroidaltaper": True, "spheroidalweightscutoff": 1e-3})
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    acc = Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt)
+    gg.grid(acc)
+    chunk = oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed,
+                         pointing=pnt)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(chunk)
+    assert gg.support()[0] == og.cache.support
+    worst = 0.0
+    for a, b in zip(og.cache.cfs, gg.convolution_functions()):
+        if a is None:
+            continue
+        worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+    assert worst < TOL, worst
+    _check_grid(og, gg)
+    wg = gg.finaliseWeights()
+    wc = og.finalise_weights()
+    assert np.max(wc) > 0
+    assert rel_l2(wg, wc) < 1e-4, rel_l2(wg, wc)
+    # finaliseGrid with the grid correction, on the GPU's own grid
+    grid = gg.grids()[0]
+    img_gpu = gg.finaliseGrid()
+    og.grids = [grid.copy()]
+    img_cpu = og.finalise_grid()
+    from oracle import cf as cfm
+    cx, cy = cfm.sph_correction_vectors(grid.shape, og.grdsf)
+    corr = (cx[:, None] * cy[None, :])[:, :, None, None]
+    safe = np.where(corr == 0, 1.0, corr)
+    assert rel_l2(img_gpu / safe, img_cpu / safe) < TOL
+    model, _ = snapped_model(ds, nx, cell, max_nu=0.5, extra=4)
+    gd = gg.clone()
+    gd.initialiseDegrid(Axes(cell, cell), model)
+    vg = np.zeros_like(ds.vis)
+    gd.degrid(Accessor(ds.uvw, ds.freq, vg, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    og.initialise_degrid(model, cell, cell)
+    vc = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=ds.noise, flag=ds.flag, feed1=feed,
+                           pointing=pnt))
+    assert np.abs(vc).max() > 0
+    assert rel_l2(vg, vc) < TOL, rel_l2(vg, vc)
+
+
 # ---- WProject parset variants ---------------------------------------------------
 # (parset keys, oracle keywords, generic keys): non-linear w-sampling
 # (PowerWSampling, GaussianWSampling), per-plane supports with peak offsets,

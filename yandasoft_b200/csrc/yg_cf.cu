@@ -555,6 +555,8 @@ struct AWScreenArgs {
   float inv_n;             // 1/(nx*ny) normalisation of the backward transform
   const double* wphase;
   float2* buf;
+  const double* tx;        // spheroidal taper per qnx / qny column (null: no taper)
+  const double* ty;
 };
 
 __global__ void k_awscreen(AWScreenArgs a, long long total) {
@@ -566,14 +568,18 @@ __global__ void k_awscreen(AWScreenArgs a, long long total) {
     const double x2 = __dmul_rn(__dmul_rn((double)x - (double)a.nx / 2, a.ccellx), __dmul_rn((double)x - (double)a.nx / 2, a.ccellx));
     const double r2 = __dadd_rn(x2, y2);
     float2 v = make_float2(0.f, 0.f);
-    if (r2 < 1.0) {
+    // the spheroidal taper is defined in the central qnx x qny region only
+    const int qix = x + a.qnx / 2 - a.nx / 2, qiy = y + a.qny / 2 - a.ny / 2;
+    const bool inq = !a.tx || (qix >= 0 && qix < a.qnx && qiy >= 0 && qiy < a.qny);
+    if (r2 < 1.0 && inq) {
+      const float taper = a.tx ? (float)__dmul_rn(a.tx[qix], a.ty[qiy]) : 1.f;
       const float so = cb_out(x, y, a.nx, a.ny);
       float2 pt = a.pattern[x + (size_t)a.nx * y];
       pt.x = __fmul_rn(pt.x * so, a.inv_n);
       pt.y = __fmul_rn(pt.y * so, a.inv_n);
-      // pattern * conj(pattern), then * taper (1)
-      const float wr = __fsub_rn(__fmul_rn(pt.x, pt.x), __fmul_rn(pt.y, -pt.y));
-      const float wi = __fadd_rn(__fmul_rn(pt.x, -pt.y), __fmul_rn(pt.y, pt.x));
+      // pattern * conj(pattern), then * taper
+      const float wr = __fmul_rn(__fsub_rn(__fmul_rn(pt.x, pt.x), __fmul_rn(pt.y, -pt.y)), taper);
+      const float wi = __fmul_rn(__fadd_rn(__fmul_rn(pt.x, -pt.y), __fmul_rn(pt.y, pt.x)), taper);
       const double phase = __dmul_rn(a.wphase[b], __dsub_rn(1.0, sqrt(__dsub_rn(1.0, r2))));
       double s, c;
       sincos(phase, &s, &c);
@@ -610,7 +616,24 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
   const size_t plane_bytes = (size_t)nx * ny * sizeof(float2);
   CF_TRY(work.ensure(plane_bytes * (nw + 1)));
   float2* pat = work.as<float2>() + (size_t)nw * nx * ny;
-  DevBuf dphase, dsup, doffs, tmp;
+  DevBuf dphase, dsup, doffs, tmp, dtaper;
+  if (p.spheroidaltaper) {
+    // AWProjectVisGridder.cc:338-354: grdsf(|q - qn/2| / (qn/2)) per column,
+    // the edge value interpolated from its neighbours
+    Spheroidal grdsf(M_PI * 3, p.alpha);
+    std::vector<double> t(qnx + qny);
+    for (int k = 0; k < 2; ++k) {
+      const int q = k ? qny : qnx;
+      double* f = t.data() + (k ? qnx : 0);
+      for (int i = 0; i < q; ++i) f[i] = grdsf(std::fabs((double)i - (double)(q / 2)) / (double)(q / 2));
+      if (q > 3) {
+        f[0] = 3.0 * (f[1] - f[2]) + f[3];
+        if (q % 2 == 1) f[q - 1] = f[0];
+      }
+    }
+    CF_TRY(dtaper.ensure(t.size() * sizeof(double)));
+    CF_TRY(cudaMemcpy(dtaper.p, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   CF_TRY(dphase.ensure(nw * sizeof(double)));
   CF_TRY(dsup.ensure(nw * sizeof(int)));
   CF_TRY(doffs.ensure(nw * sizeof(int2)));
@@ -645,7 +668,8 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
       FFT_TRY(cufftExecC2C(plan1, (cufftComplex*)pat, (cufftComplex*)pat, CUFFT_INVERSE));
       // pattern now checkerboard-signed centred inverse transform x N
       AWScreenArgs a{nx, ny, qnx, qny, ccellx, ccelly, pat, 1.f / ((float)nx * (float)ny), dphase.as<double>(),
-                     work.as<float2>()};
+                     work.as<float2>(), p.spheroidaltaper ? dtaper.as<double>() : nullptr,
+                     p.spheroidaltaper ? dtaper.as<double>() + qnx : nullptr};
       const long long total = (long long)nw * nx * ny;
       k_awscreen<<<(int)std::min<long long>((total + 255) / 256, 148 * 64), 256, 0, st>>>(a, total);
       FFT_TRY(cufftExecC2C(planw, (cufftComplex*)work.p, (cufftComplex*)work.p, CUFFT_FORWARD));

@@ -47,6 +47,7 @@ struct AWCFParams : WProjCFParams {
   int maxfields = 1;
   int nchan_cf = 1;               // channels of the cache (1 unless frequency dependent)
   std::vector<double> freqs;      // per cache channel
+  bool spheroidaltaper = false;   // anti-aliasing spheroidal taper on the image-plane screen
 };
 
 struct AWFeedJob {

@@ -307,8 +307,8 @@ void Gridder::configure(Kind k, const Parset& p, const Parset& full) {
         throw_if(maxfeeds_ <= 0, YG_ERR_ARG, "Maximum number of feeds must be one or more");
         throw_if(maxfields_ <= 0, YG_ERR_ARG, "Maximum number of fields must be one or more");
         freqdep_ = p.get_bool("frequencydependent", true);
-        throw_if(p.get_bool("spheroidaltaper", false), YG_ERR_UNSUPPORTED,
-                 "AWProject spheroidaltaper=true is not supported by this gridder");
+        aw_taper_ = p.get_bool("spheroidaltaper", false);
+        aw_weights_cutoff_ = p.get_double("spheroidalweightscutoff", 0.0);
         const std::string illum = p.get("illumination", "disk");
         throw_if(illum != "disk", YG_ERR_UNSUPPORTED, "Illumination " + illum + " is not supported (disk only)");
         diameter_ = convert_quantity(p.get("diameter"), "m");
@@ -363,6 +363,8 @@ std::unique_ptr<Gridder> Gridder::clone() const {
   g->maxfeeds_ = maxfeeds_;
   g->maxfields_ = maxfields_;
   g->freqdep_ = freqdep_;
+  g->aw_taper_ = aw_taper_;
+  g->aw_weights_cutoff_ = aw_weights_cutoff_;
   g->pointing_tol_ = pointing_tol_;
   g->pa_tol_ = pa_tol_;
   g->freq_tol_ = freq_tol_;
@@ -697,6 +699,7 @@ void Gridder::init_cf(const Chunk& dc) {
     p.nchan_cf = aw_nchan_;
     p.freqs.resize(aw_nchan_);
     for (int c = 0; c < aw_nchan_; ++c) p.freqs[c] = freqs[c];
+    p.spheroidaltaper = aw_taper_;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1115,8 +1118,9 @@ void Gridder::degrid_plan(Chunk& dc, Plan& pl) {
 // ---------------------------------------------------------------------------
 void Gridder::prepare_corrections() {
   // SphFuncVisGridder::correctConvolution factors for the padded shape; the
-  // AWProject gridder without a spheroidal taper applies none.
-  if (kind_ == Kind::AWProject) {
+  // AWProject gridder applies them only with a spheroidal taper
+  // (AWProjectVisGridder::correctConvolution).
+  if (kind_ == Kind::AWProject && !aw_taper_) {
     corr_d_.release();
     return;
   }
@@ -1191,7 +1195,27 @@ void Gridder::finalise_weights(float* out, bool out_on_device) {
       cuda_check(dout.ensure((size_t)onx * ony * np * sizeof(float)), "alloc");
       dst = dout.as<float>();
     }
-    rc_check(aw_weights_image(cf_.view(), planes, offs, wts, np, cnx, cny, nx_, ny_, onx, ony, dst, stream_),
+    // the CFs' spheroidal taper over the weights grid, values at or below
+    // spheroidalweightscutoff set to zero (AWProjectVisGridder.cc:641-664)
+    std::vector<double> taper;
+    if (aw_taper_) {
+      Spheroidal grdsf(M_PI * 3, alpha_);
+      taper.resize(cnx + cny);
+      for (int k = 0; k < 2; ++k) {
+        const int n = k ? cny : cnx, c = n / 2;
+        double* f = taper.data() + (k ? cnx : 0);
+        for (int i = 0; i < n; ++i) {
+          const double val = grdsf(std::fabs((double)i - (double)c) / (double)c);
+          f[i] = val > aw_weights_cutoff_ ? val : 0.0;
+        }
+        if (n > 3) {
+          f[0] = 3.0 * (f[1] - f[2]) + f[3];
+          if (n % 2 == 1) f[n - 1] = f[0];
+        }
+      }
+    }
+    rc_check(aw_weights_image(cf_.view(), planes, offs, wts, np, cnx, cny, nx_, ny_, onx, ony, dst, stream_,
+                              aw_taper_ ? &taper : nullptr),
              "AWProject weights");
     if (!out_on_device)
       cuda_check(cudaMemcpy(out, dst, (size_t)onx * ony * np * sizeof(float), cudaMemcpyDeviceToHost), "weights");

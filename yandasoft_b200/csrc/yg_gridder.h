@@ -206,6 +206,8 @@ class Gridder {
   // AW
   double diameter_ = 12.0, blockage_ = 2.0;
   int maxfeeds_ = 1, maxfields_ = 1;
+  bool aw_taper_ = false;               // AWProject spheroidaltaper
+  double aw_weights_cutoff_ = 0.0;      // AWProject spheroidalweightscutoff
   bool freqdep_ = true;
   double pointing_tol_ = 1e-4, pa_tol_ = 0.1, freq_tol_ = 1e-6;
   std::vector<std::vector<int>> aw_done_;          // [field][feed]

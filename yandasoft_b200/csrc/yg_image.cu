@@ -210,19 +210,27 @@ __global__ void k_aw_embed(CFView cf, const int* __restrict__ planes, const int2
 }
 
 __global__ void k_aw_accum(const float2* __restrict__ buf, const double* __restrict__ wts, int nb, int cnx, int cny,
-                           int nplanes, float* __restrict__ acc) {
+                           int nplanes, const double* __restrict__ tx, const double* __restrict__ ty,
+                           float* __restrict__ acc) {
   const long long per = (long long)cnx * cny;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nplanes; i += (long long)gridDim.x * blockDim.x) {
     const int pc = (int)(i / per);
     const long long px = i % per;
     const int x = (int)(px % cnx), y = (int)(px / cnx);
     const float sg = sgn_out(x, y, cnx, cny);
+    // a spheroidal taper of the CFs is divided out where it is positive
+    // (AWProjectVisGridder.cc:735-745); elsewhere the value is dropped
+    const float taper = tx ? (float)__dmul_rn(tx[x], ty[y]) : 1.f;
     float a = acc[i];
     for (int b = 0; b < nb; ++b) {
       const double wt = wts[(size_t)b * nplanes + pc];
       if (!(wt > 0.0)) continue;
       const float2 v = buf[(size_t)b * per + px];
-      const float vr = v.x * sg, vi = v.y * sg;
+      float vr = v.x * sg, vi = v.y * sg;
+      if (tx) {
+        vr = taper > 0.f ? __fdiv_rn(vr, taper) : 0.f;
+        vi = taper > 0.f ? __fdiv_rn(vi, taper) : 0.f;
+      }
       const float r = __fsub_rn(__fmul_rn(vr, vr), __fmul_rn(vi, -vi));
       a = (float)((double)a + wt * (double)r);
     }
@@ -284,12 +292,19 @@ __global__ void k_extract_plain(const float* __restrict__ in, int nx, int ny, fl
 
 int aw_weights_image(const CFView& cf, const std::vector<int>& planes, const std::vector<int2>& offs,
                      const std::vector<double>& wts, int nplanes, int cnx, int cny, int nx, int ny, int onx, int ony,
-                     float* out, cudaStream_t st) {
+                     float* out, cudaStream_t st, const std::vector<double>* taper) {
   const int nrows = (int)planes.size();
   const long long per = (long long)cnx * cny;
   DevBuf acc;
   IM_TRY(acc.ensure((size_t)per * nplanes * sizeof(float)));
   IM_TRY(cudaMemsetAsync(acc.p, 0, (size_t)per * nplanes * sizeof(float), st));
+  DevBuf dtaper;
+  if (taper) {
+    IM_TRY(dtaper.ensure(taper->size() * sizeof(double)));
+    IM_TRY(cudaMemcpy(dtaper.p, taper->data(), taper->size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const double* tx = taper ? dtaper.as<double>() : nullptr;
+  const double* ty = taper ? dtaper.as<double>() + cnx : nullptr;
   if (nrows > 0) {
     const int B = std::min(nrows, 32);
     DevBuf buf, dplanes, doffs, dwts;
@@ -326,7 +341,7 @@ int aw_weights_image(const CFView& cf, const std::vector<int>& planes, const std
         break;
       }
       k_aw_accum<<<blocks_for(per * nplanes), 256, 0, st>>>(buf.as<float2>(), dwts.as<double>(), B, cnx, cny, nplanes,
-                                                           acc.as<float>());
+                                                           tx, ty, acc.as<float>());
       if (cudaStreamSynchronize(st) != cudaSuccess) rc = YG_ERR_CUDA;   // host staging vectors are reused
     }
     cufftDestroy(plan);

@@ -34,9 +34,11 @@ int image_to_grids(ImageFFT& f, const float* image, int nx, int ny, int nplanes,
 
 // AWProject finaliseWeights: planes[r] = CF index of sum-of-weights row r with
 // data, offs[r] its CF offset, wts[r * nplanes + pol + npol * chan] its
-// weights; out is (onx, ony, nplanes) on the device
+// weights; out is (onx, ony, nplanes) on the device.  taper (cnx + cny
+// values, x then y), when given, is the CFs' spheroidal taper, divided out of
+// every transformed CF before its |.|^2 is summed
 int aw_weights_image(const CFView& cf, const std::vector<int>& planes, const std::vector<int2>& offs,
                      const std::vector<double>& wts, int nplanes, int cnx, int cny, int nx, int ny, int onx, int ony,
-                     float* out, cudaStream_t st);
+                     float* out, cudaStream_t st, const std::vector<double>* taper = nullptr);
 
 }  // namespace yg
