@@ -266,6 +266,48 @@ def test_awproject_spheroidal_taper(ygmod, oracle_mod):
     assert rel_l2(vg, vc) < TOL, rel_l2(vg, vc)
 
 
+def test_padding(ygmod, oracle_mod):
+    """gridder.padding = 2: the gridder works on the padded shape
+    (TableVisGridder.cc:1002, paddedShape), so its grid equals the oracle's at
+    twice the size with the same cell; finaliseGrid returns the centre of the
+    padded image and initialiseDegrid pads the model with zeros."""
+    import oracle
+    from yandasoft_b200.gridder import Accessor, Axes
+    ds = _data(duration=300.0, nchan=4)
+    nx, cell = 256, 20.0 * ARCSEC
+    params = {"wmax": _wmax(ds), "nwplanes": 9, "oversample": 4, "maxsupport": 256}
+    og, gg = make_pair("WProject", params, generic={"gridder.padding": 2.0})
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    gg.grid(Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag))
+    og.initialise_grid(2 * nx, 2 * nx, 1, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag))
+    assert gg.grids()[0].shape[:2] == (2 * nx, 2 * nx)
+    _check_grid(og, gg)
+    grid = gg.grids()[0]
+    img = gg.finaliseGrid()
+    assert img.shape[:2] == (nx, nx)
+    og.grids = [grid.copy()]
+    full = og.finalise_grid()
+    centre = full[nx // 2:nx // 2 + nx, nx // 2:nx // 2 + nx]
+    from oracle import cf as cfm
+    cx, cy = cfm.sph_correction_vectors(grid.shape, og.grdsf)
+    corr = (cx[:, None] * cy[None, :])[nx // 2:nx // 2 + nx, nx // 2:nx // 2 + nx, None, None]
+    safe = np.where(corr == 0, 1.0, corr)
+    assert rel_l2(img / safe, centre / safe) < TOL
+    model, _ = snapped_model(ds, nx, cell, max_nu=0.5, extra=4)
+    gd = gg.clone()
+    gd.initialiseDegrid(Axes(cell, cell), model)
+    vg = np.zeros_like(ds.vis)
+    gd.degrid(Accessor(ds.uvw, ds.freq, vg, noise=ds.noise, flag=ds.flag))
+    big = np.zeros((2 * nx, 2 * nx, 1, 1), dtype=np.float32, order="F")
+    big[nx // 2:nx // 2 + nx, nx // 2:nx // 2 + nx] = model
+    og.initialise_degrid(big, cell, cell)
+    vc = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=ds.noise, flag=ds.flag))
+    assert np.abs(vc).max() > 0
+    assert rel_l2(vg, vc) < TOL, rel_l2(vg, vc)
+
+
 # ---- WProject parset variants ---------------------------------------------------
 # (parset keys, oracle keywords, generic keys): non-linear w-sampling
 # (PowerWSampling, GaussianWSampling), per-plane supports with peak offsets,
