@@ -375,8 +375,9 @@ def cpu_baseline_aw(w, d, ps=None, target_s=15.0, threads=None):
     its rows phased to its own centre): the oracle's CF generation (the numpy
     restatement of AWProjectVisGridder::initConvolutionFunction) timed per
     (beam, channel) set of w-planes, and one degrid + one grid pass of its C
-    gridder on a bounded sample of that beam's rows at every 12th channel,
-    threads over row slices (one gridder each, sharing the CF cache).  With a
+    gridder on that beam's rows and channels (its whole chunk), threads over
+    row slices (one gridder each, sharing the CF cache), repeated until about
+    target_s seconds have passed.  With a
     parset `ps`, the GPU gridder grids the same sample with it and its CF
     matrices and grid are compared with the oracle's.
     Returns (Mvis/s, info)."""
@@ -385,7 +386,7 @@ def cpu_baseline_aw(w, d, ps=None, target_s=15.0, threads=None):
     threads = threads or (os.cpu_count() or 1)
     nx = w["nx"]
     cell = w["cell"] * ARCSEC
-    chans = np.arange(0, d["nchan"], 12)
+    chans = np.arange(d["nchan"])
     rows_all = np.nonzero(d["feed_np"] == 0)[0]
     freq = np.ascontiguousarray(d["freq_np"][chans])
     kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
@@ -450,13 +451,18 @@ def cpu_baseline_aw(w, d, ps=None, target_s=15.0, threads=None):
         return sub.vis.size
 
     t0 = time.perf_counter()
+    n = reps = 0
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        n = sum(ex.map(work, slices))
-    t = time.perf_counter() - t0
+        while True:
+            n += sum(ex.map(work, slices))
+            reps += 1
+            t = time.perf_counter() - t0
+            if t >= target_s or reps >= 50:
+                break
     info = dict(cores=threads, seconds=t,
-                sample="%d of %d rows (beam 0's instance), channels %s of %d, %d pols; one degrid + one grid pass; "
-                       "%d threads over row slices sharing the oracle's CF cache"
-                % (len(rows), d["nrow"], chans.tolist(), d["nchan"], d["npol"], threads),
+                sample="%d of %d rows (beam 0's instance), all %d channels, %d pols; one degrid + one grid pass, "
+                       "repeated %d times; %d threads over row slices sharing the oracle's CF cache"
+                % (len(rows), d["nrow"], d["nchan"], d["npol"], reps, threads),
                 cf={"cpu_port_s_per_beam_channel": round(t_cf / njobs, 3),
                     "cpu_port_s_all_%d_beams_x_%d_channels" % (w["nbeam"], d["nchan"]):
                         round(t_cf / njobs * w["nbeam"] * d["nchan"], 1), **check})
@@ -780,7 +786,42 @@ def e2e_b200(args, w, d, ps, axes, img):
     d2h = nvis * 8 + out.nbytes
     return {"value": round(nvis / t / 1e6, 3), "unit": "Mvis/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": round(t * 1e3, 2),
-            "path": "C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers"}
+            "path": "C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers",
+            **copy_bound(h2d, d2h)}
+
+
+def pcie_bandwidth(nbytes=1 << 30):
+    """Pinned host <-> device copy bandwidth (GB/s) of one nbytes copy each
+    way, best of three, CUDA events on the copying stream: the bound of the
+    end-to-end path's copies."""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    dv = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    best = {"h2d": 0.0, "d2h": 0.0}
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            for k in ("h2d", "d2h"):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                if k == "h2d":
+                    dv.copy_(h, non_blocking=True)
+                else:
+                    h.copy_(dv, non_blocking=True)
+                e1.record(st)
+                st.synchronize()
+                best[k] = max(best[k], nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del h, dv
+    return best
+
+
+def copy_bound(h2d, d2h):
+    """The copy-bound time (ms) of a step moving h2d bytes up and d2h down with
+    the two directions overlapped, at the measured pinned bandwidth."""
+    bw = pcie_bandwidth()
+    return {"pcie_gbs": {k: round(v, 1) for k, v in bw.items()},
+            "copy_bound_ms": round(1e3 * max(h2d / (bw["h2d"] * 1e9), d2h / (bw["d2h"] * 1e9)), 1)}
 
 
 def ctypes_ptr(t):
@@ -1036,7 +1077,8 @@ def e2e_beams(args, w, d, beams, ps, axes):
     d2h = nvis * 8 + len(host) * out.nbytes
     return {"value": round(nvis / t / 1e6, 3), "unit": "Mvis/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": round(t * 1e3, 2),
-            "path": "per beam: C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers"}
+            "path": "per beam: C-ABI initialiseDegrid+degrid+initialiseGrid+grid+finaliseGrid, pinned host buffers",
+            **copy_bound(h2d, d2h)}
 
 
 def main():

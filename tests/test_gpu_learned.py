@@ -127,6 +127,81 @@ def test_learned_cf_training_and_in_kernel_use(ygmod, oracle_mod):
     assert vis_err < 2 * e1 + 1e-4
 
 
+def test_learned_awproject_beams_and_channels(ygmod, oracle_mod):
+    """AWProject: one network for every CF plane of the cache, plane z =
+    w-plane + nw (channel + nchan beam) with inputs (w / wmax, frequency,
+    beam), the last two mapped onto [-1, 1]; trained on the gridder's own CFs
+    of two beams (0.5 deg apart) and two channels, then evaluated in the grid
+    and degrid kernels (form 1) and judged by the tabulated path."""
+    import oracle
+    from oracle import learned as L
+    from yandasoft_b200 import simulate
+    from yandasoft_b200.gridder import Accessor, AskapError, Axes
+    ds = simulate.make_dataset(duration_s=120.0, nchan=2, npol=1, seed=9, diameter_m=2000.0, freq0=800e6,
+                               freq1=1000e6)
+    feed = (np.arange(ds.nrow) % 2).astype(np.int32)
+    pnt = np.zeros((ds.nrow, 2))
+    pnt[feed == 1, 0] = 0.5 * math.pi / 180
+    wmax = float(np.max(np.abs(ds.uvw[:, 2])) * ds.freq.max() / simulate.C_LIGHT) * 1.05
+    params = {"wmax": wmax, "nwplanes": 5, "oversample": 4, "maxsupport": 256, "maxfeeds": 2,
+              "diameter": "25m", "blockage": "2m", "cutoff": 1e-3}
+    nx, cell = 512, 10.0 * ARCSEC
+    _, gg = make_pair("AWProject", params)
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    acc = Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt)
+    gg.grid(acc)
+    plain_grid = np.stack(gg.grids()).copy()
+    cfs = gg.convolution_functions()
+    os_, nw = 4, 5
+    assert len(cfs) == os_ * os_ * nw * 2 * 2
+    wterms = oracle.WSampling(nw, wmax).wterms()
+    wnorm = float(np.max(np.abs(wterms)))
+    gg.set_learned_params(L.init_params(1), 1.0)
+    p0, _ = gg.learned_params()
+    rep = gg.learned_train(ntrain=1 << 22, batch=16384, steps=20000, lr=1e-2, seed=2)
+    p1, s1 = gg.learned_params()
+
+    def cf_error(params_):
+        num = den = 0.0
+        for cfi, c in enumerate(cfs):
+            w = c.shape[0]
+            S = (w - 1) // 2
+            jx, jy = np.meshgrid(np.arange(w), np.arange(w), indexing="ij")
+            fu, fv, z = cfi % os_, (cfi // os_) % os_, cfi // (os_ * os_)
+            iw, ch, b = z % nw, (z // nw) % 2, z // (2 * nw)
+            X = L.tap_inputs(jx.ravel(), jy.ravel(), fu, fv, os_, S, wterms[iw], wnorm, freq=2.0 * ch - 1.0,
+                             beam=2.0 * b - 1.0)
+            Y = ygmod.mlp_eval(params_, X) * s1
+            pred = (Y[:, 0] + 1j * Y[:, 1]).reshape(w, w)
+            num += float(np.sum(np.abs(pred - c) ** 2))
+            den += float(np.sum(np.abs(c) ** 2))
+        return math.sqrt(num / den)
+
+    e1, e0 = cf_error(p1), cf_error(p0)
+    print("learned AWProject CF: rel L2 %.3e (untrained %.3e), %.0f ms" % (e1, e0, rep["train_ms"]))
+    assert e1 < 0.05 * e0
+    assert e1 < 5e-2
+    gl = gg.clone()
+    gl.set_cf_form(1)
+    gl.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    gl.grid(acc)
+    grid_err = rel_l2(np.stack(gl.grids()), plain_grid)
+    model, _ = snapped_model(ds, nx, cell, max_nu=0.5, extra=4)
+    vp = np.zeros_like(ds.vis)
+    vl = np.zeros_like(ds.vis)
+    for form, out in ((0, vp), (1, vl)):
+        gd = gg.clone()
+        gd.set_cf_form(form)
+        gd.initialiseDegrid(Axes(cell, cell), model)
+        gd.degrid(Accessor(ds.uvw, ds.freq, out, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    vis_err = rel_l2(vl, vp)
+    print("in-kernel learned AWProject CF: grid %.3e, degrid %.3e vs the tabulated path" % (grid_err, vis_err))
+    assert grid_err < 2 * e1 + 1e-4
+    assert vis_err < 2 * e1 + 1e-4
+    with pytest.raises(AskapError):
+        gl.set_cf_form(2)
+
+
 def test_learned_cf_continuous_in_w(ygmod, oracle_mod):
     """Trained on a table 4x denser in w, the network at the planes between
     the gridder's own planes is closer to the exact CF there than the nearest

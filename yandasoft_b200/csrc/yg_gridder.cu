@@ -380,6 +380,9 @@ std::unique_ptr<Gridder> Gridder::clone() const {
     learned_params(p);
     g->set_learned_params(p.data(), net_.scale);
     g->learn_wnorm_ = learn_wnorm_;
+    g->learn_wterm_h_ = learn_wterm_h_;
+    g->learn_fb_h_ = learn_fb_h_;
+    if (!learn_fb_h_.empty()) g->upload_learn_tables();
     g->cf_form_ = cf_form_;
   }
   if (device_ready_) {
@@ -699,6 +702,7 @@ void Gridder::init_cf(const Chunk& dc) {
     p.nchan_cf = aw_nchan_;
     p.freqs.resize(aw_nchan_);
     for (int c = 0; c < aw_nchan_; ++c) p.freqs[c] = freqs[c];
+    aw_cf_freqs_ = p.freqs;
     p.spheroidaltaper = aw_taper_;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -1336,6 +1340,7 @@ LearnedCF Gridder::learned_view() const {
   L.w16 = net_.w16.as<__half>();
   L.wterm = wterm_d_.as<double>();
   L.wnorm = learn_wnorm_;
+  L.fb = fb_d_.p ? fb_d_.as<float2>() : nullptr;
   L.scale = net_.scale;
   L.os = os_;
   return L;
@@ -1371,11 +1376,65 @@ size_t Gridder::cf_table_bytes() const {
 // Trains the network on this gridder's tabulated CFs, or (nw_train > its
 // plane count) on a denser table of nw_train planes spread linearly over the
 // same w range, built on the GPU for the purpose and released afterwards.
+void Gridder::upload_learn_tables() {
+  ensure_device();
+  cuda_check(wterm_d_.ensure(learn_wterm_h_.size() * sizeof(double)), "alloc");
+  cuda_check(fb_d_.ensure(learn_fb_h_.size() * sizeof(float2)), "alloc");
+  cuda_check(cudaMemcpy(wterm_d_.p, learn_wterm_h_.data(), learn_wterm_h_.size() * sizeof(double),
+                        cudaMemcpyHostToDevice), "up");
+  cuda_check(cudaMemcpy(fb_d_.p, learn_fb_h_.data(), learn_fb_h_.size() * sizeof(float2), cudaMemcpyHostToDevice),
+             "up");
+}
+
+// AWProject: the network learns every CF plane of the cache, plane z = w-plane
+// + nw (channel + nchan beam) with inputs (w term / wmax, frequency, beam), the
+// last two mapped linearly onto [-1, 1] over the cache's channels and beams.
+// It trains on the gridder's own cache (every beam of the one field must have
+// its CFs), not on a denser table.
+void Gridder::learned_train_aw(const LearnParams& lp, LearnReport* rep) {
+  throw_if(!cf_built_, YG_ERR_STATE, "AWProject learns its CFs after they are built (grid or degrid first)");
+  throw_if(maxfields_ != 1, YG_ERR_UNSUPPORTED, "the learned AWProject CF covers one field");
+  for (int f = 0; f < maxfeeds_; ++f)
+    throw_if(!aw_done_[0][f], YG_ERR_STATE, "the learned AWProject CF needs the CFs of every beam (maxfeeds)");
+  if (!net_.ready) rc_check(net_.init(mlp_initial_params(lp.seed), stream_), "network set-up");
+  const int nw = ws_.nwplanes, nc = aw_nchan_, nf = maxfeeds_;
+  double wn = 0.0;
+  for (int i = 0; i < nw; ++i) wn = std::max(wn, std::fabs(wterm_cf(i)));
+  learn_wnorm_ = wn > 0.0 ? wn : 1.0;
+  double f0 = 0.0, f1 = 0.0;
+  throw_if((int)aw_cf_freqs_.size() < nc, YG_ERR_STATE, "AWProject CF frequencies unknown");
+  if (nc > 1) {
+    f0 = *std::min_element(aw_cf_freqs_.begin(), aw_cf_freqs_.begin() + nc);
+    f1 = *std::max_element(aw_cf_freqs_.begin(), aw_cf_freqs_.begin() + nc);
+  }
+  learn_wterm_h_.assign((size_t)nw * nc * nf, 0.0);
+  learn_fb_h_.assign((size_t)nw * nc * nf, make_float2(0.f, 0.f));
+  for (int b = 0; b < nf; ++b)
+    for (int c = 0; c < nc; ++c)
+      for (int i = 0; i < nw; ++i) {
+        const size_t z = (size_t)i + (size_t)nw * (c + (size_t)nc * b);
+        learn_wterm_h_[z] = wterm_cf(i);
+        const float fx = f1 > f0 ? (float)(2.0 * (aw_cf_freqs_[c] - f0) / (f1 - f0) - 1.0) : 0.f;
+        const float bx = nf > 1 ? (float)(2.0 * b / (double)(nf - 1) - 1.0) : 0.f;
+        learn_fb_h_[z] = make_float2(fx, bx);
+      }
+  upload_learn_tables();
+  rc_check(net_.train(cf_.view(), wterm_d_.as<double>(), learn_wnorm_, os_, lp, learn_X_, learn_T_, stream_, rep,
+                      fb_d_.as<float2>()),
+           "training");
+  learn_X_.release();
+  learn_T_.release();
+}
+
 void Gridder::learned_train(const LearnParams& lp, int nw_train, LearnReport* rep) {
-  throw_if(kind_ != Kind::WProject && kind_ != Kind::WStackWProject, YG_ERR_UNSUPPORTED,
-           "the learned CF covers the W-projection gridders (WProject, WStackWProject)");
   throw_if(variablesupport_ || offsetsupport_, YG_ERR_UNSUPPORTED,
            "the learned CF needs one common support without offsets");
+  if (kind_ == Kind::AWProject) {
+    learned_train_aw(lp, rep);
+    return;
+  }
+  throw_if(kind_ != Kind::WProject && kind_ != Kind::WStackWProject, YG_ERR_UNSUPPORTED,
+           "the learned CF covers the W-projection gridders (WProject, WStackWProject) and AWProject");
   build_cf();
   if (!net_.ready) rc_check(net_.init(mlp_initial_params(lp.seed), stream_), "network set-up");
   const int nw = ws_.nwplanes;
@@ -1426,6 +1485,8 @@ void Gridder::set_cf_form(int form) {
   throw_if(form < 0 || form > 2, YG_ERR_ARG,
            "CF form must be 0 (tabulated), 1 (learned, tabulated planes) or 2 (learned, continuous)");
   throw_if(form != 0 && (!net_.ready || !wterm_d_.p), YG_ERR_STATE, "the learned CF has not been trained");
+  throw_if(form == 2 && kind_ == Kind::AWProject, YG_ERR_UNSUPPORTED,
+           "the continuous learned CF covers the W-projection gridders; AWProject takes form 1");
   cf_form_ = form;
 }
 

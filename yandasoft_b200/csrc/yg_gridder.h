@@ -161,6 +161,7 @@ class Gridder {
 
   // learned convolution function (no counterpart in the reference)
   void learned_train(const LearnParams& lp, int nw_train, LearnReport* rep);
+  void learned_train_aw(const LearnParams& lp, LearnReport* rep);
   void set_cf_form(int form);  // 0 tabulated, 1 learned at the tabulated planes, 2 learned continuous
   int cf_form() const { return cf_form_; }
   void learned_params(std::vector<float>& out) const;
@@ -238,7 +239,13 @@ class Gridder {
   bool cf_built_ = false;
   LearnedNet net_;
   int cf_form_ = 0;
-  DevBuf wterm_d_, wstack_d_, learn_X_, learn_T_;
+  DevBuf wterm_d_, wstack_d_, learn_X_, learn_T_, fb_d_;
+  // AWProject learned CF: network inputs per CF plane (w term; frequency and
+  // beam in [-1, 1]), kept on the host for clones
+  std::vector<double> learn_wterm_h_;
+  std::vector<float2> learn_fb_h_;
+  std::vector<double> aw_cf_freqs_;     // frequencies of the AWProject CF cache channels
+  void upload_learn_tables();
   double learn_wnorm_ = 1.0;
   LearnedCF learned_view() const;
   LearnedCF learned_view_for(const Chunk& dc, Plan& pl);

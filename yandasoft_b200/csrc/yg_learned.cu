@@ -44,8 +44,9 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
 
 // Training taps drawn uniformly over (CF index, tap inside its width) from the
 // tabulated cache; targets divided by `scale`.
-__global__ void k_mlp_make_set(CFView cf, const double* __restrict__ wterm, double wnorm, int os, float inv_scale,
-                               unsigned long long seed, long long n, float* __restrict__ X, float* __restrict__ T) {
+__global__ void k_mlp_make_set(CFView cf, const double* __restrict__ wterm, double wnorm, const float2* __restrict__ fb,
+                               int os, float inv_scale, unsigned long long seed, long long n, float* __restrict__ X,
+                               float* __restrict__ T) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const unsigned long long r0 = mix64(seed * 0x100000001B3ull + (unsigned long long)i * 3);
     const unsigned long long r1 = mix64(r0 ^ 0xD1B54A32D192ED03ull);
@@ -60,8 +61,8 @@ __global__ void k_mlp_make_set(CFView cf, const double* __restrict__ wterm, doub
     x[0] = ((float)(jx - S) + (float)fu / (float)os) * s1;
     x[1] = ((float)(jy - S) + (float)fv / (float)os) * s1;
     x[2] = (float)(wterm[plane] / wnorm);
-    x[3] = 0.f;
-    x[4] = 0.f;
+    x[3] = fb ? fb[plane].x : 0.f;
+    x[4] = fb ? fb[plane].y : 0.f;
     const float2 c = cf.data[cf.off[cfi] + jx + (long long)w * jy];
     T[2 * i] = c.x * inv_scale;
     T[2 * i + 1] = c.y * inv_scale;
@@ -412,7 +413,7 @@ int LearnedNet::init(const std::vector<float>& p0, cudaStream_t st) {
 }
 
 int LearnedNet::train(const CFView& cf, const double* wterm_d, double wnorm, int os, const LearnParams& lp,
-                      DevBuf& X, DevBuf& T, cudaStream_t st, LearnReport* rep) {
+                      DevBuf& X, DevBuf& T, cudaStream_t st, LearnReport* rep, const float2* fb_d) {
   if (!ready || lp.batch <= 0 || lp.steps < 0 || lp.ntrain <= 0) return YG_ERR_ARG;
   // target scale: the largest |tap|
   DevBuf mx;
@@ -438,8 +439,8 @@ int LearnedNet::train(const CFView& cf, const double* wterm_d, double wnorm, int
   scale = smax;
   ML_TRY(X.ensure((size_t)lp.ntrain * kMlpIn * sizeof(float)));
   ML_TRY(T.ensure((size_t)lp.ntrain * 2 * sizeof(float)));
-  k_mlp_make_set<<<148 * 8, 256, 0, st>>>(cf, wterm_d, wnorm, os, 1.f / smax, lp.seed, lp.ntrain, X.as<float>(),
-                                         T.as<float>());
+  k_mlp_make_set<<<148 * 8, 256, 0, st>>>(cf, wterm_d, wnorm, fb_d, os, 1.f / smax, lp.seed, lp.ntrain,
+                                         X.as<float>(), T.as<float>());
   YG_COUNT_LAUNCH();
   ML_TRY(cudaGetLastError());
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;

@@ -32,8 +32,9 @@ struct LearnedNet {
   long long step = 0;
   bool ready = false;
   int init(const std::vector<float>& p0, cudaStream_t st);
+  // fb_d: per CF plane (frequency, beam) network inputs, null for none
   int train(const CFView& cf, const double* wterm_d, double wnorm, int os, const LearnParams& lp, DevBuf& X,
-            DevBuf& T, cudaStream_t st, LearnReport* rep);
+            DevBuf& T, cudaStream_t st, LearnReport* rep, const float2* fb_d = nullptr);
 };
 
 // SIREN initialisation: first layer U(-1/5, 1/5), later layers

@@ -97,6 +97,7 @@ struct LearnedCF {
   const __half* w16;        // kMlpParams FP16 weights, null = tabulated CF
   const double* wterm;      // per CF plane (index cfi / os^2)
   double wnorm;             // w is divided by this
+  const float2* fb;         // per CF plane: (frequency, beam) inputs in [-1, 1]; null = (0, 0)
   float scale;              // tap = y * scale
   int os;
   const float4* ext;        // continuous form: per sorted sample of the plan (ru, rv, w / wnorm, 0); null = planes
@@ -114,8 +115,8 @@ __device__ __forceinline__ float2 mlp_tap(const float* __restrict__ ws, const Le
   x[0] = ((float)(jx - S) + (float)fu / (float)L.os) * s1;
   x[1] = ((float)(jy - S) + (float)fv / (float)L.os) * s1;
   x[2] = (float)(L.wterm[plane] / L.wnorm);
-  x[3] = 0.f;
-  x[4] = 0.f;
+  x[3] = L.fb ? L.fb[plane].x : 0.f;
+  x[4] = L.fb ? L.fb[plane].y : 0.f;
   const float2 y = mlp_eval(ws, x);
   return make_float2(y.x * L.scale, y.y * L.scale);
 }
