@@ -1014,6 +1014,11 @@ def run_beams(args, w):
         "gpu_launches_note": "graph nodes (kernels and memsets) x steps",
     }
     del cyc
+    if not args.no_learned:
+        try:
+            line["learned"] = learned_leg_aw(args, w, d, beams[0], ps, axes)
+        except Exception as e:  # the learned leg must not hide the plain result
+            line["learned"] = {"error": repr(e)}
     for x in beams:
         del x["gd"], x["gg"], x["acc"]
     torch.cuda.synchronize()
@@ -1029,6 +1034,67 @@ def run_beams(args, w):
         except Exception as e:  # the baseline must not hide the GPU result
             line["cpu_baseline"] = {"value": None, "error": repr(e)}
     print(json.dumps(line))
+
+
+def learned_leg_aw(args, w, d, beam, ps, axes):
+    """The learned CF beside the tabulated one for one beam's AWProject
+    instance: the network is trained on the gridder's own CF cache (every
+    channel's CF set, w, frequency and beam as inputs), then a degrid + grid
+    step runs with the network evaluated inside the kernels at the tabulated
+    planes (form 1) on a slice of the beam's rows.  Reports Mvis/s of both
+    forms, CF memory, the degridded-visibility error of the learned form
+    against the tabulated one, and the form kept (the learned one only within
+    1e-3 of the tabulated path)."""
+    import torch
+    from yandasoft_b200 import gridder as G
+    npol, nchan = d["npol"], d["nchan"]
+    gg0 = beam["gg"]
+    rep = gg0.learned_train(steps=args.learned_steps, seed=w["seed"] + 11)
+    nr = max(1, int(len(beam["rows"]) * args.learned_rows * 10))
+    uvw = beam["uvw"][:nr].contiguous()
+    vis = beam["vis"][:, :, :nr].contiguous()
+    acc = G.Accessor(uvw, d["freq"], vis, shape=(nr, nchan, npol))
+    img = model_image(w, beam["sky"], npol)
+    nx = w["nx"]
+    res = {}
+    for form in (0, 1):
+        gg = gg0.clone()
+        gg.set_cf_form(form)
+        gg.initialiseGrid(axes, (nx, nx, npol, 1))
+        gd = gg0.clone()
+        gd.set_cf_form(form)
+        gd.initialiseDegrid(axes, img)
+        mb = torch.zeros_like(vis)
+        accm = G.Accessor(uvw, d["freq"], mb, shape=(nr, nchan, npol))
+        plan = gg.plan(acc)
+        st = torch.cuda.ExternalStream(gg.stream_handle())
+        gd.degrid_plan(plan, accm)
+        gg.grid_plan(plan, acc)
+        gg.synchronize()
+        gd.synchronize()
+        vm = mb.clone()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        gd.degrid_plan(plan, accm)
+        gg.grid_plan(plan, acc)
+        e1.record(st)
+        torch.cuda.synchronize()
+        res[form] = (e0.elapsed_time(e1), vm)
+        del plan, gg, gd, accm, mb
+    nvis = nr * nchan * npol
+    err = float(torch.linalg.norm(res[1][1] - res[0][1]) / torch.linalg.norm(res[0][1]))
+    return {"trained_on": "the beam's CF cache: %d planes (33 w x %d channels), oversample %d"
+                          % (33 * nchan, nchan, w["oversample"]),
+            "train_steps": rep["steps"], "train_ms": round(rep["train_ms"], 1), "final_loss": rep["final_loss"],
+            "network_bytes": int(rep["network_bytes"]), "cf_table_bytes": int(rep["cf_table_bytes"]),
+            "slice": "first %d of beam 0's %d rows, all %d channels x %d pols" % (nr, len(beam["rows"]), nchan, npol),
+            "mvis_s": {"tabulated": round(nvis / (res[0][0] / 1e3) / 1e6, 3),
+                       "learned_planes": round(nvis / (res[1][0] / 1e3) / 1e6, 3)},
+            "degrid_rel_err_vs_tabulated": {"learned_planes": err}, "tolerance": 1e-3,
+            "cf_form_kept": "learned_planes" if err <= 1e-3 else
+                            "tabulated (fallback: the learned form differs from the tabulated path by more than 1e-3)"}
 
 
 def e2e_beams(args, w, d, beams, ps, axes):
