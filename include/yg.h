@@ -194,8 +194,12 @@ int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk);
  * continuous uv offset, w, frequency, beam; 4 hidden layers of 64; real and
  * imaginary part out; FP16 weights, FP32 accumulation) trained on the GPU on
  * the gridder's own tabulated CFs (WProjectVisGridder::initConvolutionFunction,
- * WProjectVisGridder.cc:435-726) and evaluated inside the grid and degrid
- * kernels in place of the table.  WProject and WStackWProject only. */
+ * WProjectVisGridder.cc:435-726, or AWProjectVisGridder::initConvolutionFunction,
+ * AWProjectVisGridder.cc:259-611) and evaluated inside the grid and degrid
+ * kernels in place of the table.  WProject, WStackWProject and AWProject; an
+ * AWProject handle trains after its CFs are built (every beam of maxfeeds seen,
+ * one field), with each plane's channel frequency and beam as the f and b
+ * inputs, and nwplanes_train is ignored for it. */
 typedef struct {
   int64_t ntrain;          /* training taps drawn from the tabulated CFs */
   int32_t batch;           /* taps per Adam step */
@@ -220,8 +224,8 @@ int32_t yg_mlp_nparams(void);
 int yg_learned_train(yg_gridder* g, const yg_learn_params* p, yg_learn_report* rep);
 /* 0: tabulated CFs (default); 1: the learned network at the tabulated offsets
  * and w planes; 2: the learned network at every sample's own fractional
- * offsets and w (continuous, no oversampling or w-plane quantisation).
- * YG_ERR_STATE before training. */
+ * offsets and w (continuous, no oversampling or w-plane quantisation; not for
+ * AWProject: YG_ERR_UNSUPPORTED).  YG_ERR_STATE before training. */
 int yg_set_cf_form(yg_gridder* g, int32_t form);
 int yg_learned_get_params(yg_gridder* g, float* params, float* scale);
 int yg_learned_set_params(yg_gridder* g, const float* params, float scale);
