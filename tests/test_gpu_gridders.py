@@ -54,12 +54,13 @@ def _check_degrid(og, gg, ds, model, cell):
     vg = np.zeros_like(ds.vis)
     gd.degrid(Accessor(ds.uvw, ds.freq, vg, noise=ds.noise, flag=ds.flag))
     og.initialise_degrid(model, cell, cell)
-    # the FFT side (model -> grids) and the tap side (grids -> visibilities) separately
+    # the FFT side (model -> grids) and the tap side (grids -> visibilities) separately;
+    # og2 is cloned before og degrids, so both start from the value og carried from gridding
     ginit = rel_l2(np.stack(gd.grids()), np.stack(og.grids))
-    vc = np.zeros_like(ds.vis)
-    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=ds.noise, flag=ds.flag))
     og2 = _clone_oracle(og)
     og2.grids = [np.asfortranarray(g) for g in gd.grids()]
+    vc = np.zeros_like(ds.vis)
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=ds.noise, flag=ds.flag))
     vt = np.zeros_like(ds.vis)
     og2.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vt, noise=ds.noise, flag=ds.flag))
     assert np.abs(vc).max() > 0
@@ -72,9 +73,11 @@ def _check_degrid(og, gg, ds, model, cell):
 
 
 def _clone_oracle(og):
+    """A copy of the oracle gridder as the reference's copy constructor makes
+    it: the carried image-frame visibility is copied (TableVisGridder.cc:156)."""
     import copy
     c = copy.copy(og)
-    c.carry = None
+    c.carry = None if og.carry is None else og.carry.copy()
     return c
 
 
