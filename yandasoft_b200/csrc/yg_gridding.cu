@@ -1164,34 +1164,44 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
         int jx = jx0;
         int row = jy0;
         int cell = origin + jx0 + Pg * jy0;
-        for (int st = 0; st < steps; st += 4) {
+        // one step of 32 taps into partial sum u
+        auto step = [&](const int u) {
+          // taps of the padding hold zeros in the table (read unconditionally,
+          // which keeps the four partial sums' loads independent); the
+          // network is evaluated only inside the CF width
+          const float2 cv = CFM == 3 ? ((jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe)
+                                                                 : make_float2(0.f, 0.f))
+                                     : cf_s[tap];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            // taps of the padding hold zeros in the table (read unconditionally,
-            // which keeps the four partial sums' loads independent); the
-            // network is evaluated only inside the CF width
-            const float2 cv = CFM == 3 ? ((jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe)
-                                                                   : make_float2(0.f, 0.f))
-                                       : cf_s[tap];
-#pragma unroll
-            for (int p = 0; p < NPOL; ++p) {
-              const float2 g = g_s[p * PG2 + cell];
-              re[u][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[u][p]));
-              im[u][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[u][p]));
-            }
-            tap += 32;
-            if (rows_per_step) {
-              cell += rows_per_step * Pg;
-              row += rows_per_step;
-            } else {
-              jx += 32;
-              const bool wrap = jx >= Wp;
-              jx = wrap ? jx - Wp : jx;
-              row += wrap ? 1 : 0;
-              cell += wrap ? 32 - Wp + Pg : 32;
-            }
+          for (int p = 0; p < NPOL; ++p) {
+            const float2 g = g_s[p * PG2 + cell];
+            re[u][p] = fmaf(cv.x, g.x, fmaf(cv.y, g.y, re[u][p]));
+            im[u][p] = fmaf(cv.y, g.x, fmaf(-cv.x, g.y, im[u][p]));
           }
+          tap += 32;
+          if (rows_per_step) {
+            cell += rows_per_step * Pg;
+            row += rows_per_step;
+          } else {
+            jx += 32;
+            const bool wrap = jx >= Wp;
+            jx = wrap ? jx - Wp : jx;
+            row += wrap ? 1 : 0;
+            cell += wrap ? 32 - Wp + Pg : 32;
+          }
+        };
+        // rows at and below the CF width hold only zero taps: the steps stop at
+        // the last one that reaches a row inside it (7 of 8 for 13-wide CFs in
+        // 16-wide planes); step st always feeds partial sum st mod 4
+        const int nst = min(steps, (wcf * Wp + 31) >> 5);
+        int st = 0;
+        for (; st + 4 <= nst; st += 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) step(u);
         }
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          if (st + u < nst) step(u);
         // values 2p (real) and 2p + 1 (imaginary) of polarisation p
         float x[2 * NPOL];
 #pragma unroll
