@@ -310,6 +310,7 @@ int yg_plan_grid(yg_gridder* g, const yg_plan* plan, const yg_chunk* chunk) {
     if (!plan) throw yg::YgError{YG_ERR_ARG, "NULL plan"};
     yg::Chunk c = to_chunk(chunk);
     if (!c.on_device) throw yg::YgError{YG_ERR_ARG, "plans need device-resident chunks"};
+    G(g).prepare_plan_cf(c);
     G(g).grid_plan(c, plan->pl);
   });
 }
@@ -321,6 +322,9 @@ int yg_plan_degrid(yg_gridder* g, yg_plan* plan, yg_chunk* chunk) {
     if (!c.on_device) throw yg::YgError{YG_ERR_ARG, "plans need device-resident chunks"};
     yg::Gridder& x = G(g);
     if (x.is_model_empty()) return;
+    // a plan made by another gridder of the same parset: this one's CFs
+    // (AWProject builds them from the chunk's beams and frequencies)
+    x.prepare_plan_cf(c);
     x.degrid_plan(c, plan->pl);
   });
 }
