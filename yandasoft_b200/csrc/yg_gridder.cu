@@ -939,45 +939,38 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
   const int K = (int)std::max(2.0, std::min(16.0, std::ceil(bytes / kPipePieceBytes)));
   const long long rows = (c.nrow + K - 1) / K;
   const int npieces = (int)((c.nrow + rows - 1) / rows);
-  std::vector<Chunk> staged(kPieceBufs);
-  auto piece_rows = [&](int k) { return std::min(rows, c.nrow - k * rows); };
-  // a degridded piece goes back on the download stream once its pass is done
-  auto download = [&](int k) {
-    const Chunk& dc = staged[k % kPieceBufs];
-    const long long r0 = k * rows, nr = piece_rows(k);
-    cuda_check(cudaMemcpy2DAsync((char*)c.vis + r0 * sizeof(float2), (size_t)c.nrow * sizeof(float2), dc.vis,
-                                 (size_t)nr * sizeof(float2), (size_t)nr * sizeof(float2), (size_t)c.nchan * c.npol,
-                                 cudaMemcpyDeviceToHost, down_stream_),
-               "download rows");
-    cuda_check(cudaEventRecord(piece_down_[k % kPieceBufs], down_stream_), "event");
-  };
-  staged[0] = stage_rows(c, 0, piece_rows(0), 0, true);
+  std::vector<Chunk> staged(2);
+  staged[0] = stage_rows(c, 0, std::min(rows, c.nrow), 0, true);
   for (int k = 0; k < npieces; ++k) {
-    const int b = k % kPieceBufs;
-    // Binning makes small synchronous copies, which would queue behind a large
-    // transfer on the copy engines: the piece is binned while no large copy is
-    // in flight, and only then do the previous piece's download and the next
-    // piece's upload start, beside this piece's pass.
+    const int b = k & 1;
+    const long long r0 = k * rows, nr = std::min(rows, c.nrow - r0);
+    if (k + 1 < npieces) {
+      // buffer b ^ 1 was last used by piece k - 1, which has finished (the
+      // passes below end on a host synchronisation); the upload waits for
+      // that piece's download (stage_rows)
+      const long long r1 = (k + 1) * rows;
+      staged[b ^ 1] = stage_rows(c, r1, std::min(rows, c.nrow - r1), b ^ 1, true);
+    }
+    // the host waits for this piece's upload (binning reads its frequencies
+    // through a synchronous copy); the next piece's upload runs on
     cuda_check(cudaEventSynchronize(piece_up_[b]), "wait upload");
     Chunk& dc = staged[b];
     init_cf(dc);
-    bin(dc, piece_plan_[k & 1]);
-    if (degridding && k > 0) download(k - 1);
-    if (k + 1 < npieces) {
-      // buffer (k + 1) mod 3 last held piece k - 2, whose pass has finished
-      // (every pass ends on a host synchronisation) and whose download the
-      // upload waits for (stage_rows)
-      staged[(k + 1) % kPieceBufs] = stage_rows(c, (k + 1) * rows, piece_rows(k + 1), (k + 1) % kPieceBufs, true);
-    }
+    bin(dc, piece_plan_[b]);
     if (degridding) {
-      degrid_plan(dc, piece_plan_[k & 1]);
+      degrid_plan(dc, piece_plan_[b]);
+      // the download runs on a stream of its own, beside the next upload
       cuda_check(cudaEventRecord(piece_done_, stream_), "event");
       cuda_check(cudaStreamWaitEvent(down_stream_, piece_done_, 0), "wait degrid");
+      cuda_check(cudaMemcpy2DAsync((char*)c.vis + r0 * sizeof(float2), (size_t)c.nrow * sizeof(float2), dc.vis,
+                                   (size_t)nr * sizeof(float2), (size_t)nr * sizeof(float2),
+                                   (size_t)c.nchan * c.npol, cudaMemcpyDeviceToHost, down_stream_),
+                 "download rows");
+      cuda_check(cudaEventRecord(piece_down_[b], down_stream_), "event");
     } else {
-      grid_plan(dc, piece_plan_[k & 1]);
+      grid_plan(dc, piece_plan_[b]);
     }
   }
-  if (degridding) download(npieces - 1);
   cuda_check(cudaStreamSynchronize(copy_stream_), "pieces");
   if (degridding) cuda_check(cudaStreamSynchronize(down_stream_), "pieces");
 }

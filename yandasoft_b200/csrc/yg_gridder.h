@@ -260,13 +260,12 @@ class Gridder {
   };
   static constexpr double kPipeMinBytes = 256.0 * (1 << 20);   // smaller chunks go in one piece
   static constexpr double kPipePieceBytes = 1024.0 * (1 << 20);
-  static constexpr int kPieceBufs = 3;   // an upload never waits for the download of the piece before
-  Staging staging_[kPieceBufs];
+  Staging staging_[2];
   Plan piece_plan_[2];
   cudaStream_t copy_stream_ = nullptr;   // uploads
   cudaStream_t down_stream_ = nullptr;   // downloads of degridded pieces (the other PCIe direction)
-  cudaEvent_t piece_up_[kPieceBufs] = {};
-  cudaEvent_t piece_down_[kPieceBufs] = {};
+  cudaEvent_t piece_up_[2] = {nullptr, nullptr};
+  cudaEvent_t piece_down_[2] = {nullptr, nullptr};
   cudaEvent_t piece_done_ = nullptr;
   bool pipelined(const Chunk& c) const;
   Chunk stage_rows(const Chunk& c, long long r0, long long nr, int b, bool need_vis);
