@@ -445,6 +445,44 @@ def test_psf_gridder(ygmod, oracle_mod):
     _check_grid(og, gg)
 
 
+@pytest.mark.parametrize("case", ["frequency_independent", "psf_first_beam"])
+def test_awproject_variants(ygmod, oracle_mod, case):
+    """AWProject with frequencydependent = false (one CF set per beam, at the
+    chunk's first frequency, indexed without the channel) and the PSF gridder
+    (CFs without the beam-offset slope, only the rows of the first row's beam
+    and pointing gridded unless alldatapsf)."""
+    import oracle
+    from yandasoft_b200.gridder import Accessor, Axes
+    ds = _data(duration=120.0, nchan=3, seed=9, diameter=2000.0, f0=900e6, f1=1000e6)
+    feed = (np.arange(ds.nrow) % 2).astype(np.int32)
+    pnt = np.zeros((ds.nrow, 2))
+    pnt[feed == 1, 0] = 0.5 * math.pi / 180
+    nx, cell = 512, 10.0 * ARCSEC
+    params = {"wmax": _wmax(ds), "nwplanes": 5, "oversample": 4, "maxsupport": 256, "maxfeeds": 2,
+              "diameter": "25m", "blockage": "2m", "cutoff": 1e-3}
+    psf = case == "psf_first_beam"
+    if not psf:
+        params["frequencydependent"] = False
+    og, gg = make_pair("AWProject", params)
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1), dopsf=psf)
+    gg.grid(Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    og.initialise_grid(nx, nx, 1, 1, cell, cell, dopsf=psf)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed,
+                         pointing=pnt))
+    assert gg.support()[0] == og.cache.support
+    worst = 0.0
+    n = 0
+    for a, b in zip(og.cache.cfs, gg.convolution_functions()):
+        if a is None:
+            continue
+        n += 1
+        worst = max(worst, float(np.max(np.abs(a - b)) / np.max(np.abs(a))))
+    assert n > 0 and worst < TOL, worst
+    if not psf:
+        assert len(og.cache.cfs) == 16 * 5 * 2
+    _check_grid(og, gg)
+
+
 def test_mfs_weights(ygmod, oracle_mod):
     import oracle
     from yandasoft_b200.gridder import Accessor, Axes
