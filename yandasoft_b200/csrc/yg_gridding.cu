@@ -624,13 +624,18 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             } else {
               c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
             }
+            // every polarisation's cell is loaded before any is stored (they are
+            // distinct cells), so the loads are in flight together
+            float2 g[NPOL];
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + c2];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
-              float2 g = acc_s[p * PG2 + c2];
-              g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
-              g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
-              acc_s[p * PG2 + c2] = g;
+              g[p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g[p].x));
+              g[p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g[p].y));
             }
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + c2] = g[p];
             cell += PgR;
             tap += WpR;
           }
@@ -646,13 +651,16 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             const float2 c = CFM == 3 ? ((live[q] && jx < wcf && jy < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe)
                                                                            : make_float2(0.f, 0.f))
                                       : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
+            float2 g[NPOL];
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + cell];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) {
-              float2 g = acc_s[p * PG2 + cell];
-              g.x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g.x));
-              g.y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g.y));
-              acc_s[p * PG2 + cell] = g;
+              g[p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g[p].x));
+              g[p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g[p].y));
             }
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + cell] = g[p];
           }
         }
       }
