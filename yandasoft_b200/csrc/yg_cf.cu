@@ -648,8 +648,6 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
   cufftSetStream(planw, st);
   int rc = YG_OK;
   const int ncfplanes = nw * p.maxfeeds * p.maxfields * p.nchan_cf;
-  std::vector<int> sup_dev;       // what dsup / doffs hold
-  std::vector<int2> offs_dev;
   for (const AWFeedJob& j : jobs) {
     for (int chan = 0; chan < p.nchan_cf && rc == YG_OK; ++chan) {
       const double freq = p.freqs[chan];
@@ -718,25 +716,15 @@ int cf_build_aw(CFCacheDev& cache, const AWCFParams& p, const std::vector<AWFeed
         for (int iw = 0; iw < nw; ++iw) cache.h_offsets[z0 + iw] = offs[iw];
         CF_TRY(cudaMemcpyAsync(cache.offsets.as<int2>() + z0, offs.data(), nw * sizeof(int2), cudaMemcpyHostToDevice, st));
       }
-      // the per-plane supports and offsets go up only when they change (with
-      // one common support, once): the copies from pageable memory would
-      // otherwise hold the host until the stream drains, job after job; every
-      // buffer a job reuses is ordered on the stream
-      bool same = sup_dev.size() == sup.size() && offs_dev.size() == offs.size();
-      for (size_t i = 0; same && i < sup.size(); ++i)
-        same = sup_dev[i] == sup[i] && offs_dev[i].x == offs[i].x && offs_dev[i].y == offs[i].y;
-      if (!same) {
-        CF_TRY(cudaMemcpyAsync(dsup.p, sup.data(), nw * sizeof(int), cudaMemcpyHostToDevice, st));
-        CF_TRY(cudaMemcpyAsync(doffs.p, offs.data(), nw * sizeof(int2), cudaMemcpyHostToDevice, st));
-        sup_dev = sup;
-        offs_dev = offs;
-      }
+      CF_TRY(cudaMemcpyAsync(dsup.p, sup.data(), nw * sizeof(int), cudaMemcpyHostToDevice, st));
+      CF_TRY(cudaMemcpyAsync(doffs.p, offs.data(), nw * sizeof(int2), cudaMemcpyHostToDevice, st));
       CutArgs c{work.as<float2>(), nx, ny, os, z0, dsup.as<int>(), doffs.as<int2>(), cache.off.as<long long>(),
                 cache.data.as<float2>(), (float)(os * os), inv};
       const int cs = 2 * cache.support + 1;
       dim3 g((cs * cs + 255) / 256, os * os, nw);
       k_cut<<<g, 256, 0, st>>>(c, nw, cs);
       CF_TRY(cudaGetLastError());
+      CF_TRY(cudaStreamSynchronize(st));
     }
     if (rc) break;
   }
