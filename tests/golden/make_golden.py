@@ -9,6 +9,11 @@ here).  Small seeded cases, so the fixtures stay a few tens of kB:
                         CF support and the central taps of three CF planes; the
                         gridded values at the 64 largest cells; the sum of
                         weights; degridded visibilities of a 3-point model.
+  awproject_small.npz   AWProject, 2 beams 0.5 deg apart (25 m dishes, 2 m
+                        blockage), 2 channels, 5 w-planes, oversample 4, 512^2
+                        at 10": the CF support and the central taps of three CF
+                        planes, the gridded values at the 64 largest cells, the
+                        grid's L2 norm and the sums of weights.
   sphfunc_full_pol.npz  SphFunc, the ImageFFTEquationTest::testFullPol setup:
                         degridded 4-pol visibilities of a centred point
                         (1, 0.01, -0.01, 0.9) at 40 seeded uvw.
@@ -67,6 +72,35 @@ def make_wproject(path):
                         degrid=vis.astype(np.complex64))
 
 
+def awproject_case():
+    from yandasoft_b200 import simulate
+    ds = simulate.make_dataset(duration_s=60.0, dt_s=10.0, nchan=2, seed=43, diameter_m=2000.0)
+    feed = (np.arange(ds.nrow) % 2).astype(np.int32)
+    pnt = np.zeros((ds.nrow, 2))
+    pnt[feed == 1, 0] = 0.5 * math.pi / 180
+    wmax = float(np.max(np.abs(ds.uvw[:, 2])) * ds.freq.max() / simulate.C_LIGHT) * 1.05
+    params = dict(wmax=wmax, nwplanes=5, oversample=4, maxsupport=256, maxfeeds=2, cutoff=1e-3)
+    return ds, feed, pnt, params, 512, 10.0 * ARCSEC
+
+
+def make_awproject(path):
+    import oracle
+    ds, feed, pnt, params, nx, cell = awproject_case()
+    og = oracle.OracleGridder("AWProject", diameter=25.0, blockage=2.0, **params)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed,
+                         pointing=pnt))
+    grid = og.grids[0][:, :, 0, 0]
+    s = og.cache.support
+    top = np.argsort(np.abs(grid).ravel(order="F"))[::-1][:64]
+    cfs = og.cache.cfs
+    pick = [0, len(cfs) // 2, len(cfs) - 1]
+    np.savez_compressed(path, support=np.int32(s), cf_pick=np.array(pick, dtype=np.int32),
+                        cf_centre=np.stack([cfs[k][s - 2:s + 3, s - 2:s + 3] for k in pick]).astype(np.complex64),
+                        grid_cells=top.astype(np.int64), grid_values=grid.ravel(order="F")[top].astype(np.complex64),
+                        grid_l2=np.float64(np.linalg.norm(grid)), sumw=og.sumw.astype(np.float64))
+
+
 def full_pol_case():
     npix = 512
     img = np.zeros((npix, npix, 4, 1), dtype=np.float32, order="F")
@@ -95,6 +129,7 @@ if __name__ == "__main__":
     import oracle
     oracle.build()
     make_wproject(os.path.join(HERE, "wproject_small.npz"))
+    make_awproject(os.path.join(HERE, "awproject_small.npz"))
     make_full_pol(os.path.join(HERE, "sphfunc_full_pol.npz"))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):

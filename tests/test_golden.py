@@ -55,3 +55,22 @@ def test_oracle_reproduces_full_pol_golden(oracle_mod):
     # the known answer of ImageFFTEquationTest::testFullPol, to 1e-5
     for p, v in enumerate([1.0, 0.01, -0.01, 0.9]):
         assert np.max(np.abs(gold["vis"][:, :, p] - v)) < 1e-5
+
+
+def test_oracle_reproduces_awproject_golden(oracle_mod):
+    import make_golden as mg
+    import oracle
+    gold = np.load(os.path.join(HERE, "golden", "awproject_small.npz"))
+    ds, feed, pnt, params, nx, cell = mg.awproject_case()
+    og = oracle.OracleGridder("AWProject", diameter=25.0, blockage=2.0, **params)
+    og.initialise_grid(nx, nx, 1, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed,
+                         pointing=pnt))
+    s = og.cache.support
+    assert s == int(gold["support"])
+    for i, k in enumerate(gold["cf_pick"]):
+        c = og.cache.cfs[k]
+        assert np.max(np.abs(c[s - 2:s + 3, s - 2:s + 3] - gold["cf_centre"][i])) <= 1e-6 * np.max(np.abs(c))
+    grid = og.grids[0][:, :, 0, 0].ravel(order="F")
+    assert _rel(grid[gold["grid_cells"]], gold["grid_values"]) < 1e-6
+    assert np.array_equal(og.sumw, gold["sumw"])

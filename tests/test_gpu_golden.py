@@ -64,3 +64,25 @@ def test_sphfunc_full_pol_against_golden(ygmod):
     vis = np.zeros((uvw.shape[0], 2, 4), dtype=np.complex64, order="F")
     g.degrid(Accessor(uvw, freq, vis))
     assert np.max(np.abs(vis - gold["vis"])) <= TOL
+
+
+def test_awproject_against_golden(ygmod):
+    import make_golden as mg
+    from yandasoft_b200.gridder import Accessor, Axes, VisGridderFactory
+    gold = np.load(os.path.join(HERE, "golden", "awproject_small.npz"))
+    ds, feed, pnt, params, nx, cell = mg.awproject_case()
+    ps = {"gridder": "AWProject", "gridder.AWProject.diameter": "25m", "gridder.AWProject.blockage": "2m",
+          **{"gridder.AWProject.%s" % k: v for k, v in params.items()}}
+    g = VisGridderFactory.make(ps)
+    g.initialiseGrid(Axes(cell, cell), (nx, nx, 1, 1))
+    g.grid(Accessor(ds.uvw, ds.freq, ds.vis, noise=ds.noise, flag=ds.flag, feed1=feed, pointing=pnt))
+    s = g.support()[0]
+    assert s == int(gold["support"])
+    cfs = g.convolution_functions()
+    for i, k in enumerate(gold["cf_pick"]):
+        c = cfs[k]
+        assert np.max(np.abs(c[s - 2:s + 3, s - 2:s + 3] - gold["cf_centre"][i])) <= TOL * np.max(np.abs(c))
+    grid = g.grids()[0][:, :, 0, 0].ravel(order="F")
+    assert _rel(grid[gold["grid_cells"]], gold["grid_values"]) < TOL
+    assert abs(np.linalg.norm(grid) - float(gold["grid_l2"])) <= TOL * float(gold["grid_l2"])
+    assert np.array_equal(g.sum_weights(), gold["sumw"])
