@@ -285,6 +285,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def max_over_ranks(ms, dist=None, device="cuda"):
+    """The job's time for the timed steps: the slowest rank's (every rank
+    takes part in the reduction)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, nvis_per_rank, ms_step):
+    """Whole-job throughput (Mvis/s): every replica processes its own copy of
+    the workload (weak scaling), the job takes the slowest rank's time."""
+    return world * nvis_per_rank / (ms_step / 1e3) / 1e6
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -554,15 +571,13 @@ def run_b200(args, w):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = G.kernel_launch_count() - launches0
+    ms = max_over_ranks(ms, dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     k1 = gg.kernel_times()
     k1d = gd.kernel_times()
     ms_step = ms / args.steps
-    value = world * nvis / (ms_step / 1e3) / 1e6
+    value = job_value(world, nvis, ms_step)
     kgrid_ms = (k1["kgrid_ms"] - k0["kgrid_ms"]) / max(1.0, k1["kgrid_calls"] - k0["kgrid_calls"])
     kdeg_ms = (k1d["kdegrid_ms"] - k0d["kdegrid_ms"]) / max(1.0, k1d["kdegrid_calls"] - k0d["kdegrid_calls"])
     nvalid_vis = info["nvalid"] * npol
