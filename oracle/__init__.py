@@ -325,10 +325,13 @@ class OracleGridder:
                 self.cache = cfmod.awproject_cf(self.uvcell[0], self.uvcell[1], p, chunk.freq, feeds, centre,
                                                 is_psf=self.psf)
                 self.aw_params = p
-                if self.sumw is None:
-                    n = p.nwplanes * p.maxfeeds * p.maxfields * self.aw_nchan
-                    rows = n * self.os * self.os if self.track_per_os else n
-                    self.sumw = np.zeros((rows, self.npol, self.nchan_img), dtype=np.float64, order="F")
+            if self.sumw is None:
+                # AWProjectVisGridder's sums of weights have a row per CF plane
+                # (initialiseSumOfWeights, after every initialiseGrid)
+                p = self.aw_params
+                n = p.nwplanes * p.maxfeeds * p.maxfields * self.aw_nchan
+                rows = n * self.os * self.os if self.track_per_os else n
+                self.sumw = np.zeros((rows, self.npol, self.nchan_img), dtype=np.float64, order="F")
         self._flat = self.cache.flatten()
 
     # ---- index maps -------------------------------------------------------
