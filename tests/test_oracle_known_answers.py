@@ -38,3 +38,26 @@ def test_full_pol_degrid_sphfunc(oracle_mod):
     out = vis - before
     for p, v in enumerate(vals):
         assert np.max(np.abs(out[:, :, p] - v)) < 1e-5
+
+
+def test_awproject_sums_of_weights_after_reinitialised_grid(oracle_mod):
+    """An AWProject gridder that grids a PSF pass and then a plain pass (the
+    reverse sequence of TableVisGridderTest) keeps its CF cache and gets
+    fresh sums of weights with a row per CF plane at each initialiseGrid."""
+    import math
+
+    import numpy as np
+    from yandasoft_b200 import simulate
+    ds = simulate.make_dataset(duration_s=30.0, nchan=2, seed=5, diameter_m=2000.0)
+    wmax = float(np.max(np.abs(ds.uvw[:, 2])) * ds.freq.max() / simulate.C_LIGHT) * 1.05
+    og = oracle_mod.OracleGridder("AWProject", wmax=wmax, nwplanes=5, oversample=1, maxsupport=128, maxfeeds=1,
+                                  diameter=25.0, blockage=2.0, cutoff=1e-3)
+    cell = 20 * math.pi / (180 * 3600)
+    chunk = oracle_mod.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=ds.noise, flag=ds.flag)
+    totals = []
+    for psf in (True, False):
+        og.initialise_grid(256, 256, 1, 1, cell, cell, dopsf=psf)
+        og.grid(chunk)
+        assert og.sumw.shape == (5 * 2, 1, 1)
+        totals.append(og.sumw.sum())
+    assert totals[0] == totals[1] > 0
