@@ -84,12 +84,42 @@ def _setup(L):
     L.orc_last_error.restype = ctypes.c_char_p
     L.orc_wstack_wproj_map.restype = I32
     L.orc_wstack_wproj_map.argtypes = [I64, I32, P, P, I32, D, I32, I32, D, P, P]
+    L.orc_set_tap_kernels.restype = None
+    L.orc_set_tap_kernels.argtypes = [P, P]
     L.orc_dft.restype = I32
     L.orc_dft.argtypes = [I64, I32, P, P, I32, P, P, P, I32]
 
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+REF_GRIDKERNEL = os.path.join(_HERE, "_ref", "libref_gridkernel.so")
+_REF = None
+
+
+def reference_gridkernel():
+    """The reference's own GridKernel.cc compiled by oracle/Makefile into
+    oracle/_ref (None when it was not built: the reference tree is absent)."""
+    global _REF
+    if _REF is None and os.path.exists(REF_GRIDKERNEL):
+        _REF = ctypes.CDLL(REF_GRIDKERNEL)
+        _REF.ref_grid_kernel_info.restype = I32
+        _REF.ref_grid_kernel_info.argtypes = [ctypes.c_char_p, I32]
+    return _REF
+
+
+def use_reference_gridkernel(on: bool = True):
+    """Makes the generic loop call the reference's compiled GridKernel::grid /
+    degrid (on) or the restated tap loops (off, the default)."""
+    L = lib()
+    if not on:
+        L.orc_set_tap_kernels(None, None)
+        return
+    R = reference_gridkernel()
+    if R is None:
+        raise OracleError("oracle/_ref/libref_gridkernel.so is not built (the reference tree is absent)")
+    L.orc_set_tap_kernels(ctypes.cast(R.ref_grid_kernel, P), ctypes.cast(R.ref_degrid_kernel, P))
 
 
 class OracleError(RuntimeError):
@@ -262,7 +292,9 @@ class OracleGridder:
         self._init_axes(nx, ny, npol, nchan, cell_x, cell_y, freq_axis)
         self.psf = dopsf
         self.forward = False
-        self.grids = [np.zeros((nx, ny, npol, nchan), dtype=np.complex64, order="F") for _ in range(self._ngrids())]
+        n = nx * ny * npol * nchan
+        buf = np.zeros(n * self._ngrids(), dtype=np.complex64)
+        self.grids = [buf[i * n:(i + 1) * n].reshape((nx, ny, npol, nchan), order="F") for i in range(self._ngrids())]
         self._init_sumw()
         self.first_psf_row = True
         self.rep_feed = None
@@ -393,10 +425,8 @@ class OracleGridder:
         freq = np.ascontiguousarray(chunk.freq, dtype=np.float64)
         delay = None if chunk.delay is None else np.ascontiguousarray(chunk.delay, dtype=np.float64)
         assert chunk.vis.flags.f_contiguous and chunk.vis.dtype == np.complex64
-        grids = np.stack([g for g in self.grids], axis=0) if len(self.grids) > 1 else self.grids[0]
-        grids = np.asfortranarray(grids) if len(self.grids) == 1 else grids
         # grids buffer: ngrids consecutive column-major (nx, ny, npol, nchan) blocks
-        gbuf = np.concatenate([g.ravel(order="F") for g in self.grids])
+        gbuf = self._grid_buffer()
         sumw = self.sumw if self.sumw is not None else np.zeros((1, self.npol, self.nchan_img), order="F")
         st = _Stats()
         _check(lib().orc_generic(ctypes.byref(cfg), nrow, nchan, npol, _p(uvw), _p(delay), _p(freq), _p(chan_map),
@@ -409,6 +439,19 @@ class OracleGridder:
                                                                  order="F")
         self.stats = st
         return st
+
+    def _grid_buffer(self):
+        """The grids as one buffer of consecutive column-major blocks: the
+        grids themselves when they are already such views of one array (as
+        initialise_grid makes them), else a copy."""
+        n = self.nx * self.ny * self.npol * self.nchan_img
+        g0 = self.grids[0]
+        base = g0.base if g0.base is not None else g0
+        if (base.ndim == 1 and base.dtype == np.complex64 and base.size == n * len(self.grids)
+                and all(g.flags.f_contiguous and g.dtype == np.complex64 and g.size == n
+                        and g.ctypes.data == base.ctypes.data + i * n * 8 for i, g in enumerate(self.grids))):
+            return base
+        return np.concatenate([g.ravel(order="F") for g in self.grids])
 
     def _psf_mask(self, chunk: Chunk):
         if self.kw.get("alldatapsf", False):

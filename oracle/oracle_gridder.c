@@ -315,6 +315,21 @@ static void orc_degrid_kernel(float *out, const float *grid, int nx, const float
     out[1] = im;
 }
 
+/* The tap loops the generic loop calls: the restatements above by default;
+ * the checker may install the reference's own compiled GridKernel
+ * (oracle/_ref) through orc_set_tap_kernels to pin them (NULL restores
+ * the restatements). */
+typedef void (*orc_grid_fn)(float *, int, const float *, float, float, int, int, int);
+typedef void (*orc_degrid_fn)(float *, const float *, int, const float *, int, int, int);
+static orc_grid_fn orc_grid_tap = orc_grid_kernel;
+static orc_degrid_fn orc_degrid_tap = orc_degrid_kernel;
+
+void orc_set_tap_kernels(orc_grid_fn g, orc_degrid_fn d)
+{
+    orc_grid_tap = g ? g : orc_grid_kernel;
+    orc_degrid_tap = d ? d : orc_degrid_kernel;
+}
+
 /* ---------------------------------------------------------------------- */
 /* TableVisGridder::generic                                               */
 /* ---------------------------------------------------------------------- */
@@ -448,7 +463,7 @@ int orc_generic(const orc_cfg *cfg, int64_t nrow, int nchan, int npol,
                     grid = grids + 2 * ((int64_t)g_ind * grid_elems + plane_cells * (pol + (int64_t)cfg->npol * img_chan));
                     if (cfg->forward) {
                         float cv[2], re, im;
-                        orc_degrid_kernel(cv, grid, cfg->nx, cf, iuo, ivo, support);
+                        orc_degrid_tap(cv, grid, cfg->nx, cf, iuo, ivo, support);
                         st->samples += 1.0;
                         st->taps += (double)((2 * support + 1) * (2 * support + 1));
                         if (mfs) { cv[0] *= mfs[ch]; cv[1] *= mfs[ch]; }
@@ -475,14 +490,14 @@ int orc_generic(const orc_cfg *cfg, int64_t nrow, int nchan, int npol,
                             float ri = ph_re * vi + ph_im * vr;
                             rr *= wt; ri *= wt;
                             if (mfs) { rr *= mfs[ch]; ri *= mfs[ch]; }
-                            orc_grid_kernel(grid, cfg->nx, cf, rr, ri, iuo, ivo, support);
+                            orc_grid_tap(grid, cfg->nx, cf, rr, ri, iuo, ivo, support);
                             st->samples += 1.0;
                             st->taps += (double)((2 * support + 1) * (2 * support + 1));
                             *sw += wt;
                         } else if (!psf_ok || psf_ok[i]) {
                             float ur = 1.f * wt, ui = 0.f * wt;
                             if (mfs) { ur *= mfs[ch]; ui *= mfs[ch]; }
-                            orc_grid_kernel(grid, cfg->nx, cf, ur, ui, iuo, ivo, support);
+                            orc_grid_tap(grid, cfg->nx, cf, ur, ui, iuo, ivo, support);
                             st->samples += 1.0;
                             st->taps += (double)((2 * support + 1) * (2 * support + 1));
                             *sw += wt;
