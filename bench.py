@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--cycles", type=int, default=5, help="config 3: major cycles timed")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity leg (1% row subset against the oracle)")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
     ap.add_argument("--tile", type=int, default=0, help="uv tile side (0 = automatic)")
     ap.add_argument("--variant", type=int, default=0, help="k_grid thread layout variant (0 = automatic)")
@@ -314,77 +315,101 @@ def peaks():
 # --------------------------------------------------------------------------
 # CPU baseline (oracle restatement), bounded sample
 # --------------------------------------------------------------------------
+class CpuBaseline:
+    """The oracle's C restatement of TableVisGridder::generic timed on a row
+    subset of the same workload: one degrid + one grid pass per run.  Threads
+    run independent gridders over channel slices, as the reference
+    parallelises (one gridder clone per thread); each holds its own grids, so
+    the thread count is capped by host memory.  Every gridder, its grids
+    (zeroed and touched) and its chunk are made before the timed region; a
+    run times only the two passes.  The degridding grids are shared and left
+    zero: the tap loop does the same work whatever the cell values."""
+
+    def __init__(self, w, d, target_s=15.0, threads=None):
+        import oracle
+        import psutil
+        threads = threads or (os.cpu_count() or 1)
+        self.w, self.d = w, d
+        nx = w["nx"]
+        cell = w["cell"] * ARCSEC
+        kind = w["gridder"]
+        kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
+                  maxsupport=w["maxsupport"])
+        if kind == "WStackWProject":
+            kw["nwstacks"] = w["nwstacks"]
+        g0 = oracle.OracleGridder(kind, **kw)
+        g0.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+        g0.init_cf()
+        self.grid_bytes = sum(g.nbytes for g in g0.grids)
+        self.support = int(g0.cache.support)
+        avail = psutil.virtual_memory().available
+        mem_threads = int((0.6 * avail - self.grid_bytes) // max(1, self.grid_bytes))
+        self.threads = threads = max(1, min(threads, mem_threads))
+        nrow_all = d["nrow"]
+        freq = d["freq_np"]
+        # calibrate a row count: ~1.2 ns per tap per polarisation per pass, two passes
+        taps = (2 * g0.cache.support + 1) ** 2
+        per_sample = 2 * taps * d["npol"] * 1.2e-9 / threads
+        nrows = int(min(nrow_all, max(1000, target_s / (per_sample * len(freq)))))
+        step = max(1, nrow_all // nrows)
+        rows = np.arange(0, nrow_all, step)[:nrows]
+        uvw = np.ascontiguousarray(d["uvw_np"][rows])
+        vis = d["vis"][:, :, torch_index(rows)].cpu().numpy()          # [pol][chan][row]
+        cube = np.asfortranarray(np.transpose(vis, (2, 1, 0)))
+        self.jobs = []
+        for ch in np.array_split(np.arange(len(freq)), threads):
+            if len(ch) == 0:
+                continue
+            gd = oracle.OracleGridder(kind, **kw)
+            gd._init_axes(nx, nx, d["npol"], 1, cell, cell, None)   # initialise_degrid without the FFTs
+            gd.psf = False
+            gd.model_empty = False
+            gd.sumw = None
+            gd._init_sumw()
+            gd.grids = g0.grids
+            gd.cache, gd._flat = g0.cache, g0._flat
+            gg = oracle.OracleGridder(kind, **kw)
+            gg.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
+            gg._grid_buffer()[:] = 0                                # touch every page now
+            gg.cache, gg._flat = g0.cache, g0._flat
+            sub = np.asfortranarray(cube[:, ch, :])
+            fch = np.ascontiguousarray(freq[ch])
+            self.jobs.append((gd, gg, oracle.Chunk(uvw=uvw, freq=fch, vis=np.zeros_like(sub)),
+                              oracle.Chunk(uvw=uvw, freq=fch, vis=sub)))
+        self.sample = ("%d of %d rows (every %d-th), all %d channels x %d pols; one degrid + one grid pass; %d "
+                       "threads over channel slices, each with its own %.1f GB of grids (made before timing)"
+                       % (len(rows), nrow_all, step, len(freq), d["npol"], threads, self.grid_bytes / 1e9))
+
+    def run(self):
+        """One degrid + grid pass of every thread's gridders; (Mvis/s, seconds)."""
+        import concurrent.futures as cf
+
+        def work(job):
+            gd, gg, cd, cg = job
+            gd.degrid(cd)
+            gg.grid(cg)
+            return cg.vis.size
+
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=len(self.jobs)) as ex:
+            n = sum(ex.map(work, self.jobs))
+        t = time.perf_counter() - t0
+        return n / t / 1e6, t
+
+
 def cpu_baseline(w, d, target_s=15.0, threads=None):
-    """Times the oracle's C restatement of TableVisGridder::generic on a row
-    subset of the same workload: one degrid + one grid pass.  Threads run
-    independent gridders over channel slices, as the reference parallelises
-    (one gridder clone per thread); each holds its own grids, so the thread
-    count is capped by host memory.  The degridding grids are shared and left
-    zero: the tap loop does the same work whatever the cell values.
-    Returns (Mvis/s, info)."""
-    import concurrent.futures as cf
-    import oracle
-    import psutil
-    threads = threads or (os.cpu_count() or 1)
-    nx = w["nx"]
-    cell = w["cell"] * ARCSEC
-    kind = w["gridder"]
-    kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
-              maxsupport=w["maxsupport"])
-    if kind == "WStackWProject":
-        kw["nwstacks"] = w["nwstacks"]
-    g0 = oracle.OracleGridder(kind, **kw)
-    g0.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
-    g0.init_cf()
-    grid_bytes = sum(g.nbytes for g in g0.grids)
-    avail = psutil.virtual_memory().available
-    mem_threads = int((0.5 * avail - grid_bytes) // max(1, grid_bytes))
-    threads = max(1, min(threads, mem_threads))
-    shared = g0.grids
-    nrow_all = d["nrow"]
-    freq = d["freq_np"]
-    vis_all = d["vis"]
-    # calibrate a row count: ~2 ns per tap per pass, two passes
-    taps = (2 * g0.cache.support + 1) ** 2
-    per_sample = 2 * taps * d["npol"] * 2.0e-9 / max(1, threads)
-    nrows = int(min(nrow_all, max(1000, target_s / (per_sample * len(freq)))))
-    step = max(1, nrow_all // nrows)
-    rows = np.arange(0, nrow_all, step)[:nrows]
-    uvw = np.ascontiguousarray(d["uvw_np"][rows])
-    vis = vis_all[:, :, rows].cpu().numpy()          # [pol][chan][row]
-    cube = np.asfortranarray(np.transpose(vis, (2, 1, 0)))
-    slices = np.array_split(np.arange(len(freq)), threads)
-
-    def work(ch):
-        if len(ch) == 0:
-            return 0
-        gd = oracle.OracleGridder(kind, **kw)
-        gd._init_axes(nx, nx, d["npol"], 1, cell, cell, None)   # initialise_degrid without the FFTs
-        gd.psf = False
-        gd.sumw = None
-        gd._init_sumw()
-        gd.grids = shared
-        gd.cache = g0.cache
-        gd._flat = g0._flat
-        sub = np.asfortranarray(cube[:, ch, :])
-        out = np.zeros_like(sub)
-        gd.degrid(oracle.Chunk(uvw=uvw, freq=freq[ch], vis=out))
-        del gd
-        gg = oracle.OracleGridder(kind, **kw)
-        gg.initialise_grid(nx, nx, d["npol"], 1, cell, cell)
-        gg.cache = g0.cache
-        gg._flat = g0._flat
-        gg.grid(oracle.Chunk(uvw=uvw, freq=freq[ch], vis=sub))
-        return sub.size
-
-    t0 = time.perf_counter()
-    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        n = sum(ex.map(work, slices))
-    t = time.perf_counter() - t0
-    return n / t / 1e6, dict(cores=threads, rows=len(rows), nvis=int(n), seconds=t,
-                             sample="%d of %d rows (every %d-th), all %d channels x %d pols; one degrid + one grid "
-                                    "pass; %d threads over channel slices, each with its own %.1f GB of grids"
-                             % (len(rows), nrow_all, step, len(freq), d["npol"], threads, grid_bytes / 1e9))
+    """All host threads (one gridder per channel slice), then one thread on a
+    smaller subset.  Returns (Mvis/s, info)."""
+    cb = CpuBaseline(w, d, target_s=target_s, threads=threads)
+    cb.run()                      # warm (first touch of the CF cache and the data)
+    v, t = cb.run()
+    info = dict(cores=cb.threads, seconds=t, sample=cb.sample)
+    del cb
+    one = CpuBaseline(w, d, target_s=target_s / 3.0, threads=1)
+    v1, t1 = one.run()
+    info["single_core"] = {"value": round(v1, 4), "unit": "Mvis/s", "cores": 1, "seconds": round(t1, 2),
+                           "sample": one.sample}
+    return v, info
 
 
 def cpu_baseline_aw(w, d, ps=None, target_s=15.0, threads=None):
@@ -494,6 +519,66 @@ def torch_index(a):
 # --------------------------------------------------------------------------
 # arms
 # --------------------------------------------------------------------------
+def roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak, peak_kind, sm_hz, cf_bytes):
+    """Roofline of the dominant kernel (k_grid) and of k_degrid_t, per launch
+    (one grid or degrid pass over the workload).  The binding roofline time is
+    t_roof = max(algorithmic HBM bytes / measured HBM bandwidth,
+    8 flops per tap x taps / FP32 peak at the sampled SM clock); frac =
+    t_roof / kernel time.  Algorithmic HBM bytes of a grid pass: every on-grid
+    sample's visibility (8 B) and weight (4 B), uvw (24 B per row), flags
+    (1 B per row and channel), one write of every grid plane (8 B per cell)
+    and one read of the CF cache; of a degrid pass: one read of every grid
+    plane, every sample's visibility written (8 B), uvw and the CF cache."""
+    taps = (2 * support + 1) ** 2
+    nrowchan = d["nrow"] * d["nchan"]
+    planes = w.get("nwstacks", 1) if w["gridder"] in ("WStack", "WStackWProject") else 1
+    grid_bytes = planes * w["nx"] * w["nx"] * npol * 8.0
+    hbm_grid = nvalid_vis * 12.0 + d["nrow"] * 24.0 + nrowchan * 1.0 + grid_bytes + cf_bytes
+    hbm_degrid = grid_bytes + nvalid_vis * 8.0 + d["nrow"] * 24.0 + cf_bytes
+    flops = 8.0 * taps * nvalid_vis
+    fp32_peak = 148 * 128 * 2 * sm_hz                      # FMA lanes x 2 flops at the sampled clock
+    smem_peak = 148 * 128 * sm_hz                          # bytes per second, 128 B per clock per SM
+
+    def one(ms, hbm_bytes, smem_per_tap):
+        t = ms / 1e3
+        t_hbm = hbm_bytes / (hbm_peak * 1e9)
+        t_fp = flops / fp32_peak
+        out = {"ms": round(ms, 4), "t_roof_ms": round(1e3 * max(t_hbm, t_fp), 4),
+               "bound": "fp32" if t_fp >= t_hbm else "hbm",
+               "frac": round(max(t_hbm, t_fp) / t, 4) if t > 0 else 0.0,
+               "fp32": {"achieved_tflops": round(flops / t / 1e12, 3) if t > 0 else 0.0,
+                        "peak_tflops": round(fp32_peak / 1e12, 2), "frac": round(t_fp / t, 4) if t > 0 else 0.0},
+               "hbm": {"bytes": int(hbm_bytes), "achieved_gbs": round(hbm_bytes / t / 1e9, 2) if t > 0 else 0.0,
+                       "peak_gbs": hbm_peak, "peak_kind": peak_kind, "frac": round(t_hbm / t, 4) if t > 0 else 0.0},
+               "smem": {"bytes_per_tap": smem_per_tap,
+                        "frac": round(nvalid_vis / npol * taps * smem_per_tap / smem_peak / t, 4) if t > 0 else 0.0}}
+        return out
+
+    g = one(kgrid_ms, hbm_grid, 16.0 * npol + 8.0)
+    dg = one(kdeg_ms, hbm_degrid, 8.0 * npol + 8.0)
+    traffic = kgrid_traffic(info, support, npol)
+    return {"bound": g["bound"], "kernel": "k_grid", "achieved": g["fp32"]["achieved_tflops"],
+            "peak": g["fp32"]["peak_tflops"], "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 flops) at the "
+                                                           "sampled SM clock",
+            "unit": "TFLOP/s", "frac": g["frac"], "traffic": traffic,
+            "traffic_note": "DRAM bytes per k_grid launch, scaled from a single-kernel ncu capture of a small slice "
+                            "of this workload by samples and work items",
+            "t_roof_ms": g["t_roof_ms"], "kgrid_ms": round(kgrid_ms, 4), "kdegrid_ms": round(kdeg_ms, 4),
+            "k_grid": g, "k_degrid_t": dg, "taps_per_s": round(taps * nvalid_vis / (kgrid_ms / 1e3), 1)
+            if kgrid_ms > 0 else 0,
+            "note": "t_roof = max(algorithmic HBM bytes / measured HBM bandwidth, 8 flops x taps / FP32 peak); "
+                    "frac = t_roof / kernel time; smem frac: the named shared-memory bytes per tap and sample "
+                    "over 128 B per clock per SM"}
+
+
+def kgrid_traffic(info, support, npol):
+    """DRAM bytes of one k_grid launch, from the per-sample and per-item rates
+    of an ncu capture of a slice of the same workload: the sorted records and
+    visibilities read per sample, the padded tiles written per item."""
+    pad = info["tile"] + 2 * support
+    return int(48.9 * info["nvalid"] + 0.84 * info["nitems"] * npol * pad * pad * 8)
+
+
 def run_b200(args, w):
     import torch
     from yandasoft_b200 import build
@@ -582,24 +667,10 @@ def run_b200(args, w):
     kdeg_ms = (k1d["kdegrid_ms"] - k0d["kdegrid_ms"]) / max(1.0, k1d["kdegrid_calls"] - k0d["kdegrid_calls"])
     nvalid_vis = info["nvalid"] * npol
     taps = (2 * support + 1) ** 2
-    # algorithmic HBM bytes of one k_grid launch: read each on-grid sample's
-    # visibilities once, write the (padded-tile) scratch once.
     hbm_peak, peak_kind = peaks()
-    alg_bytes = nvalid_vis * 8.0 + info["nvalid"] * (4 + 4 + 4) + 0.0
-    achieved_gbs = alg_bytes / (kgrid_ms / 1e3) / 1e9 if kgrid_ms > 0 else 0.0
-    flops = 8.0 * taps * nvalid_vis
     sm_hz = (clk.summary().get("sm_mhz") or 1965.0) * 1e6
-    fp32_peak_tflops = 148 * 128 * 2 * sm_hz / 1e12
-    # the binding resource of k_grid: shared memory, 16 B read-modify-write of
-    # the cell per tap and polarisation plus the 8 B CF tap, against 128 B per
-    # clock per SM
-    smem_bytes = info["nvalid"] * taps * (16.0 * npol + 8.0)
-    smem_peak = 148 * 128 * sm_hz
-    smem_tbs = smem_bytes / (kgrid_ms / 1e3) / 1e12 if kgrid_ms > 0 else 0.0
-    # measured on a slice of config 1: 48.9 B read per sample (record + sorted
-    # visibilities), 0.84 of the padded-tile scratch written
-    pad = info["tile"] + 2 * support
-    traffic = int(48.9 * info["nvalid"] + 0.84 * info["nitems"] * npol * pad * pad * 8)
+    roof = roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak, peak_kind, sm_hz,
+                    gg.cf_bytes())
     line = {
         "metric": METRIC,
         "cf_form": "plain (tabulated CF)",
@@ -613,22 +684,7 @@ def run_b200(args, w):
                    "l2": "inputs (%.1f GB of visibilities) larger than L2" % (nvis * 8 / 1e9),
                    "step": "one degrid pass + one grid pass over all samples, inputs resident in HBM",
                    "plan_build_s": round(t_plan, 3), "autotune": tune},
-        "roofline": {"bound": "hbm", "kernel": "k_grid", "achieved": round(achieved_gbs, 2),
-                     "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved_gbs / hbm_peak, 4), "traffic": traffic,
-                     "traffic_note": "DRAM bytes per k_grid launch, scaled by samples and items from an ncu "
-                                     "capture of a 2% slice (profiles/k_grid_k_degrid_t_config1_small.md)",
-                     "kgrid_ms": round(kgrid_ms, 4), "kdegrid_ms": round(kdeg_ms, 4),
-                     "binding": {"resource": "shared memory", "achieved": round(smem_tbs, 3),
-                                 "peak": round(smem_peak / 1e12, 3), "unit": "TB/s",
-                                 "frac": round(smem_tbs * 1e12 / smem_peak, 4),
-                                 "note": "per tap: 16 B cell read-modify-write per polarisation + 8 B CF; "
-                                         "148 SMs x 128 B per clock at the sampled SM clock (nominal, not measured)"},
-                     "fp32": {"achieved_tflops": round(flops / (kgrid_ms / 1e3) / 1e12, 3) if kgrid_ms > 0 else 0,
-                              "peak_tflops_at_sampled_clock": round(fp32_peak_tflops, 2),
-                              "frac": round(flops / (kgrid_ms / 1e3) / 1e12 / fp32_peak_tflops, 4) if kgrid_ms > 0 else 0,
-                              "note": "8 flops per tap per sample; 148 SMs x 128 FP32 lanes x 2 at the sampled SM clock"},
-                     "taps_per_s": round(taps * nvalid_vis / (kgrid_ms / 1e3), 1) if kgrid_ms > 0 else 0},
+        "roofline": roof,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
     }
@@ -642,17 +698,121 @@ def run_b200(args, w):
             line["learned"] = {"error": repr(e)}
     if not args.no_e2e:
         line["e2e"] = e2e_b200(args, w, d, ps, axes, img)
+    if rank == 0 and not args.no_parity and w["gridder"] in ("WProject", "WStackWProject"):
+        try:
+            line["parity"] = parity_subset(w, d, ps, axes, img)
+        except Exception as e:  # the parity leg must not hide the GPU result
+            line["parity"] = {"error": repr(e)}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             v, inf = cpu_baseline(w, d)
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
-                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2)}
+                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2),
+                                    "single_core": inf.get("single_core")}
         except Exception as e:  # the baseline must not hide the GPU result
             line["cpu_baseline"] = {"value": None, "error": repr(e)}
     if dist:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def dft_model(img, cell, uvw, freq, rows, chans):
+    """FP64 direct DFT of the model image's pixels (polarisation 0) at the
+    given (row, channel) samples: V = sum_k S_k exp(+2 pi i f/c (u l + v m +
+    w (n - 1))) with l, m the pixel offsets from the image centre (the
+    measurement equation of UnpolarizedPointSource::calcPoint)."""
+    import torch
+    nx = img.shape[0]
+    xs, ys = np.nonzero(img[:, :, 0, 0])
+    flux = torch.tensor(img[xs, ys, 0, 0].astype(np.float64), device="cuda")
+    lm = torch.tensor(np.stack([(xs - nx // 2) * cell, (ys - nx // 2) * cell], 1), device="cuda")
+    nn = torch.sqrt(1 - lm[:, 0] ** 2 - lm[:, 1] ** 2) - 1
+    U = torch.as_tensor(np.asarray(uvw)[rows], device="cuda")
+    f = torch.tensor(np.asarray(freq)[chans], device="cuda")
+    ph = 2 * math.pi * (f / C_LIGHT)[:, None] * (U[:, 0:1] * lm[None, :, 0] + U[:, 1:2] * lm[None, :, 1]
+                                                 + U[:, 2:3] * nn[None, :])
+    return (flux[None] * torch.exp(1j * ph)).sum(1).cpu().numpy()
+
+
+def parity_subset(w, d, ps, axes, img, frac=0.01, seed=20240):
+    """The timed workload's parity on a seeded row subset (1% of the rows,
+    every channel and polarisation): the GPU gridder, with the tile and
+    kernel choice of the timed run, against the oracle's restatement of the
+    reference gridder on the same samples.  Grid: relative L2 error over every
+    w-stack, sums of weights compared exactly, index mismatches (cell, CF
+    index and status of every sample).  Degrid of the model image: the oracle
+    degrids the GPU's own transformed grids (the tap path), relative L2 error
+    of the visibilities; each degrid result's error against the FP64 DFT of
+    the model on a sample of 4096 gridded points (polarisation 0) is stated."""
+    import torch
+    import oracle
+    from yandasoft_b200 import gridder as G
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    nrow_all, nchan, npol = d["nrow"], d["nchan"], d["npol"]
+    rows = np.sort(rng.choice(nrow_all, max(1, int(nrow_all * frac)), replace=False))
+    nr = len(rows)
+    uvw = np.ascontiguousarray(d["uvw_np"][rows])
+    freq = d["freq_np"]
+    vis_dev = d["vis"][:, :, torch_index(rows)].contiguous()          # [pol][chan][row]
+    cube = np.asfortranarray(np.transpose(vis_dev.cpu().numpy(), (2, 1, 0)))
+    nx = w["nx"]
+    cell = w["cell"] * ARCSEC
+    acc = G.Accessor(torch.from_numpy(uvw).cuda(), d["freq"], vis_dev, shape=(nr, nchan, npol))
+    gg = G.VisGridderFactory.make(ps)
+    gg.initialiseGrid(axes, (nx, nx, npol, 1))
+    plan = gg.plan(acc)
+    gg.grid_plan(plan, acc)
+    iu, iv, cfi, st = plan.samples(gg, acc)
+    kw = dict(nwplanes=w["nwplanes"], wmax=d["wmax"], oversample=w["oversample"], cutoff=w["cutoff"],
+              maxsupport=w["maxsupport"])
+    if w["gridder"] == "WStackWProject":
+        kw["nwstacks"] = w["nwstacks"]
+    og = oracle.OracleGridder(w["gridder"], **kw)
+    og.initialise_grid(nx, nx, npol, 1, cell, cell)
+    og.grid(oracle.Chunk(uvw=uvw, freq=freq, vis=cube))
+    S = og.cache.support
+    oiu, oiv, ofu, ofv = oracle.indices(uvw, freq, og.uvcell[0], og.uvcell[1], og.os, nx, nx)
+    cmap, gmap = og._maps(oracle.Chunk(uvw=uvw, freq=freq, vis=cube))
+    gmap = np.zeros_like(cmap) if gmap is None else gmap
+    okp = (cmap >= 0) & (gmap >= 0)
+    on = okp & (oiu - S > 0) & (oiv - S > 0) & (oiu + S < nx) & (oiv + S < nx)
+    ocfi = ofu + og.os * (ofv + og.os * cmap.astype(np.int64))
+    mism = int((st != np.where(~okp, 1, np.where(on, 3, 2))).sum() + (iu[on] != oiu[on]).sum()
+               + (iv[on] != oiv[on]).sum() + (cfi[on] != ocfi[on]).sum())
+    num = den = 0.0
+    for a, b in zip(gg.grids(), og.grids):
+        num += float(np.linalg.norm((a - b).ravel()) ** 2)
+        den += float(np.linalg.norm(b.ravel()) ** 2)
+    sumw_equal = bool(np.array_equal(gg.sum_weights(), og.sumw))
+    tile = plan.info()["tile"]
+    gd = gg.clone()
+    del gg
+    gd.initialiseDegrid(axes, img)
+    out = torch.zeros_like(vis_dev)
+    accm = G.Accessor(acc.uvw, acc.freq, out, shape=(nr, nchan, npol))
+    gd.degrid_plan(plan, accm)
+    vg = accm.vis_numpy()
+    og.grids = [np.asfortranarray(g) for g in gd.grids()]
+    del gd, plan
+    og.model_empty = False
+    og.carry = None
+    vc = np.zeros_like(cube)
+    og.degrid(oracle.Chunk(uvw=uvw, freq=freq, vis=vc))
+    og.grids = None
+    vis_rel = float(np.linalg.norm((vg - vc).ravel()) / np.linalg.norm(vc.ravel()))
+    r, c = np.nonzero(on)
+    k = rng.choice(len(r), min(4096, len(r)), replace=False)
+    dft = dft_model(img, cell, uvw, freq, r[k], c[k])
+    e_dft = lambda v: float(np.linalg.norm(v[r[k], c[k], 0] - dft) / np.linalg.norm(dft))
+    torch.cuda.empty_cache()
+    return {"subset": "%d of %d rows (seeded %.0f%%), all %d channels x %d pols; tile %d as timed"
+                      % (nr, nrow_all, 100 * frac, nchan, npol, tile),
+            "grid_rel": math.sqrt(num / den) if den > 0 else None, "vis_rel": vis_rel, "index_mismatch": mism,
+            "sumw_equal": sumw_equal, "tolerance": 1e-5,
+            "degrid_rel_err_vs_dft": {"gpu": e_dft(vg), "oracle": e_dft(vc), "samples": int(len(k))},
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def learned_leg(args, w, d, ps, axes, img):
@@ -790,7 +950,7 @@ def e2e_b200(args, w, d, ps, axes, img):
 
     step()   # warm (CF generation, allocations)
     torch.cuda.synchronize()
-    k = max(1, min(args.steps, 3))
+    k = max(1, args.steps)
     t0 = time.perf_counter()
     for _ in range(k):
         step()
@@ -864,22 +1024,38 @@ def run_reference(args, w):
         raise SystemExit("the reference arm needs the same synthetic generator (GPU)")
     times = []
     vals = []
-    for s in range(args.warmup + args.steps):
-        if w["gridder"] == "AWProject":
+    if w["gridder"] == "AWProject":
+        for s in range(args.warmup + args.steps):
             v, inf = cpu_baseline_aw(w, d, target_s=8.0)
-        else:
-            v, inf = cpu_baseline(w, d, target_s=8.0)
-        if s >= args.warmup:
-            vals.append(v)
-            times.append(inf["seconds"])
+            if s >= args.warmup:
+                vals.append(v)
+                times.append(inf["seconds"])
+        cores, sample, support = inf["cores"], inf["sample"], None
+    else:
+        # gridders, grids and chunks made once; each step times one degrid +
+        # grid pass of every thread's gridders
+        cb = CpuBaseline(w, d, target_s=8.0)
+        for s in range(args.warmup + args.steps):
+            v, t = cb.run()
+            if s >= args.warmup:
+                vals.append(v)
+                times.append(t)
+        cores, sample, support = cb.threads, cb.sample, cb.support
     value = float(np.mean(vals))
+    npol = d["npol"]
+    cfg = {"workload": w["name"], "gridder": w["gridder"], "vis_samples": int(d["nrow"] * d["nchan"] * npol),
+           "rows": int(d["nrow"]), "channels": d["nchan"], "pols": npol, "grid": [w["nx"], w["nx"], npol, 1],
+           "oversample": w["oversample"]}
+    if support is not None:
+        cfg.update(support=support, taps_per_sample=(2 * support + 1) ** 2)
+    cfg["step"] = "one degrid pass + one grid pass over a bounded row sample of the workload, on the host cores"
     line = {"metric": METRIC, "impl": "reference",
             "value": round(value, 4), "unit": "Mvis/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * float(np.mean(times)), 2), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": w["name"], "gridder": w["gridder"]},
-            "cpu_baseline": {"value": round(value, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
-                             "sample": inf["sample"]},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; see bench.py workload())",
+            "config": cfg,
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mvis/s", "cores": cores, "kind": "port",
+                             "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "Mvis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -1056,7 +1232,8 @@ def run_beams(args, w):
             v, inf = cpu_baseline_aw(w, d, ps)
             line["cf_cache"].update(inf["cf"])
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mvis/s", "cores": inf["cores"], "kind": "port",
-                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2)}
+                                    "sample": inf["sample"], "seconds": round(inf["seconds"], 2),
+                                    "single_core": inf.get("single_core")}
         except Exception as e:  # the baseline must not hide the GPU result
             line["cpu_baseline"] = {"value": None, "error": repr(e)}
     print(json.dumps(line))

@@ -3,10 +3,10 @@
  *
  * A drop-in GPU back end for yandasoft's IVisGridder path
  * (askap/gridding/IVisGridder.h:64-140) for the SphFunc, WProject, WStack and
- * AWProject gridders, plus a W-stacking + W-projection hybrid.  The C++
- * IVisGridder shim that a yandasoft maintainer adds
- * unpacks its accessor into a yg_chunk and forwards each virtual call to the
- * function named beside it below.
+ * AWProject gridders, plus a W-stacking + W-projection hybrid.  A C++
+ * IVisGridder subclass on the yandasoft side unpacks its accessor into a
+ * yg_chunk and forwards each virtual call to the function named beside it
+ * below.
  *
  * Conventions
  *   - Every function returns 0 (YG_OK) or a YG_ERR_* code; yg_last_error()
@@ -90,7 +90,10 @@ int yg_clone(const yg_gridder* g, yg_gridder** out);
 
 void yg_destroy(yg_gridder* g);
 
-/* IVisGridder::initialiseGrid (TableVisGridder.cc:997-1030). */
+/* IVisGridder::initialiseGrid (TableVisGridder.cc:997-1030).  dopsf: grid the
+ * weights (PSF); dopcf: the preconditioner function (weights without the MFS
+ * factor, conjugate CF on one half of the uv plane, no sums of weights,
+ * TableVisGridder.cc:825-851); not both at once. */
 int yg_initialise_grid(yg_gridder* g, const yg_axes* axes, int32_t nx, int32_t ny, int32_t npol, int32_t nchan,
                        int32_t dopsf, int32_t dopcf);
 
@@ -164,7 +167,11 @@ int yg_set_tile(yg_gridder* g, int32_t tile);      /* 0 = automatic */
 int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
 /* k_grid thread layout: 0 or 1 the default, 2 and 3 halve / quarter the tap
  * threads (each steps down twice / four times the rows); YG_ERR_UNSUPPORTED
- * at the next grid call when the CF width has no such layout */
+ * at the next grid call when the CF width has no such layout.  Adding 16
+ * keeps each thread's running tap sums in registers while consecutive
+ * samples cover the same cell (layouts of at most 8 rows per thread); adding
+ * 32 as well orders each tile's samples by position before CF for gridding
+ * (plans made afterwards keep both orders) and reads the taps through L2. */
 int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */
@@ -172,21 +179,25 @@ int yg_get_stream(yg_gridder* g, void** stream);
 
 /* ---- degridding without device allocation ----
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
- * code that records its major cycle into a CUDA graph while a stream is being
- * captured (device allocation cannot be captured), or an application that
- * fixes the GPU's memory budget at start-up and forbids later allocations.
+ * an application that fixes each GPU's memory budget when it starts and
+ * forbids any later allocation (so that a long-running imaging service cannot
+ * fail half way through a major cycle for lack of memory), or a host
+ * framework whose own pool allocator owns the device's memory.
  * Same semantics as yg_degrid for a device-resident chunk (on_device = 1):
  * the model visibilities are added into chunk->vis.  The gridder must have
  * its convolution functions built (yg_build_cf, or one earlier yg_degrid) and
  * its model grid initialised (yg_initialise_degrid); both stay owned by the
- * handle.  Every temporary of the call lives in one static device array of
- * about 60 MB that each GPU loading the library holds until exit; the call
- * takes at most 2^20 rows x channels (YG_ERR_ARG beyond that), 1, 2 or 4
- * polarisations and 65536 channels, and allocates nothing.  The array's
- * device address is looked up the first time the call runs on a device, so
- * make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (other streams, other host threads)
- * race on it and must be serialised by the caller. */
+ * handle.  SphFunc, WStack, WProject and WStackWProject with the tabulated
+ * CFs; AWProject (CFs built per chunk) and the learned CF forms return
+ * YG_ERR_UNSUPPORTED.  Every temporary of the call lives in one static device
+ * array of about 60 MB that each GPU loading the library holds until exit;
+ * the call takes at most 2^20 rows x channels (YG_ERR_ARG beyond that), 1, 2
+ * or 4 polarisations and 65536 channels, and allocates nothing.  The array's
+ * device address is looked up the first time the call runs on a device.  All
+ * calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race on it and must be serialised by the caller.  Like
+ * yg_degrid, the call reads the chunk's frequencies back to the host and
+ * waits for the handle's stream before it returns. */
 int yg_degrid_noalloc(yg_gridder* g, yg_chunk* chunk);
 
 /* ---- learned convolution function ----
@@ -253,6 +264,19 @@ int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y);
 typedef struct yg_cycle yg_cycle;
 int yg_cycle_create(int32_t n, yg_gridder* const* degridders, yg_gridder* const* gridders, const yg_chunk* chunks,
                     yg_cycle** out);
+/* The same with the other roles of ImageFFTEquation::calcImagingEquations
+ * (ImageFFTEquation.cc:362-387, 437-479): after the residual, instance i's
+ * PSF gridder (yg_initialise_grid with dopsf = 1) and preconditioner-function
+ * gridder (dopcf = 1), where given, grid the same visibility buffer within
+ * the same graph branch.  model and residual are required; psf and pcf may
+ * be NULL. */
+typedef struct yg_cycle_roles {
+  yg_gridder* model;      /* degrids the model (after yg_initialise_degrid) */
+  yg_gridder* residual;   /* grids the residual (after yg_initialise_grid) */
+  yg_gridder* psf;        /* PSF gridder or NULL */
+  yg_gridder* pcf;        /* preconditioner-function gridder or NULL */
+} yg_cycle_roles;
+int yg_cycle_create_roles(int32_t n, const yg_cycle_roles* roles, const yg_chunk* chunks, yg_cycle** out);
 /* replays the graph `cycles` times; *gpu_ms (may be NULL) receives the GPU time */
 int yg_cycle_run(yg_cycle* c, int32_t cycles, float* gpu_ms);
 /* nodes of the recorded graph */

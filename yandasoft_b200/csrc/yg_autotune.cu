@@ -71,7 +71,9 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   std::vector<int> vmaxes = {def_vmax};
   for (int v : {def_vmax / 4, def_vmax * 4})
     if (v >= 128 && v <= (1 << 20)) vmaxes.push_back(v);
-  const std::vector<int> variants = {1, 2};
+  // thread layouts: the default, half the threads; then the default with
+  // register accumulation, and with position-major records (taps through L2)
+  const std::vector<int> variants = {1, 2, 17, 49};
   const int save_tile = tile_override_, save_vmax = vmax_, save_mode = grid_mode_;
   Chunk scratch_chunk = dc;
   DevBuf model;
@@ -123,11 +125,14 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
     }
     if (t == def_tile && vm == def_vmax && v == 1) rep.default_ms = ms;
   };
-  // first the tile and the thread layout at the default work-item size (the
-  // default itself first), then the work-item size around the best of those
-  for (int v : variants)
-    for (int t : tiles)
-      if (trials < max_trials) trial(t, def_vmax, v);
+  // first the tile with the default layout and work-item size (the default
+  // itself first), then the other layouts at the best tile, then the
+  // work-item size around the best of those
+  for (int t : tiles)
+    if (trials < max_trials) trial(t, def_vmax, variants[0]);
+  const int lead_tile = rep.best.tile;
+  for (size_t k = 1; k < variants.size(); ++k)
+    if (trials < max_trials && lead_tile > 0) trial(lead_tile, def_vmax, variants[k]);
   const TuneChoice lead = rep.best;
   for (int vm : vmaxes)
     if (vm != def_vmax && trials < max_trials && lead.tile > 0) trial(lead.tile, vm, lead.variant);

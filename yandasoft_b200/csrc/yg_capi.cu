@@ -357,7 +357,9 @@ int yg_set_tile(yg_gridder* g, int32_t tile) {
 
 int yg_set_grid_variant(yg_gridder* g, int32_t variant) {
   return guarded([&] {
-    if (variant < 0 || variant > 3) throw yg::YgError{YG_ERR_ARG, "variant must be 0 to 3"};
+    if (variant < 0 || (variant & ~48) > 3)
+      throw yg::YgError{YG_ERR_ARG,
+                        "variant must be 0 to 3, plus 16 (register accumulation) and 32 (position-major records)"};
     G(g).set_grid_mode(variant);
   });
 }
@@ -497,6 +499,26 @@ int yg_cycle_create(int32_t n, yg_gridder* const* degridders, yg_gridder* const*
     }
     auto c = std::make_unique<yg_cycle>();
     c->b.build(dg, gg, ch);
+    *out = c.release();
+  });
+}
+
+int yg_cycle_create_roles(int32_t n, const yg_cycle_roles* roles, const yg_chunk* chunks, yg_cycle** out) {
+  return guarded([&] {
+    if (n <= 0 || !roles || !chunks || !out) throw yg::YgError{YG_ERR_ARG, "NULL argument"};
+    std::vector<yg::Gridder*> dg(n), gg(n), psf(n, nullptr), pcf(n, nullptr);
+    std::vector<yg::Chunk> ch(n);
+    bool any_psf = false, any_pcf = false;
+    for (int i = 0; i < n; ++i) {
+      if (!roles[i].model || !roles[i].residual) throw yg::YgError{YG_ERR_ARG, "every instance needs a model and a residual gridder"};
+      dg[i] = &G(roles[i].model);
+      gg[i] = &G(roles[i].residual);
+      if (roles[i].psf) { psf[i] = &G(roles[i].psf); any_psf = true; }
+      if (roles[i].pcf) { pcf[i] = &G(roles[i].pcf); any_pcf = true; }
+      ch[i] = to_chunk(&chunks[i]);
+    }
+    auto c = std::make_unique<yg_cycle>();
+    c->b.build(dg, gg, ch, any_psf ? psf : std::vector<yg::Gridder*>{}, any_pcf ? pcf : std::vector<yg::Gridder*>{});
     *out = c.release();
   });
 }

@@ -1,7 +1,9 @@
 // Major cycle as a CUDA graph: for each of n imaging instances (a degridder
-// holding the model, a gridder for the residual, one device-resident chunk of
-// observed visibilities), degrid the model into model visibilities, subtract
-// them from the observed ones and grid the residual
+// holding the model, a gridder for the residual, optionally a PSF gridder and
+// a preconditioner-function gridder, one device-resident chunk of observed
+// visibilities), degrid the model into model visibilities, subtract them from
+// the observed ones and grid the residual, then the PSF and the
+// preconditioner function from the same buffer
 // (ImageFFTEquation::calcImagingEquations, ImageFFTEquation.cc:437-479).
 // The instances are recorded once, each on a branch of its own (eight side
 // streams, fork/join events), into one graph that every later cycle replays
@@ -54,12 +56,18 @@ void CycleBatch::enqueue(Instance& in, cudaStream_t st) {
   k_subtract<<<std::max(1, blocks), 256, 0, st>>>(in.obs.vis, in.model_vis.as<float2>(), in.resid_vis.as<float2>(), n);
   ck(cudaGetLastError(), "subtract");
   in.gg->grid_enqueue(in.resid, in.plan, in.mfs_gg, st);
+  // the PSF and the preconditioner grid the weights of the same buffer
+  if (in.psf) in.psf->grid_enqueue(in.resid, in.psf_plan, in.mfs_psf, st);
+  if (in.pcf) in.pcf->grid_enqueue(in.resid, in.pcf_plan, in.mfs_pcf, st);
 }
 
 void CycleBatch::build(const std::vector<Gridder*>& dgs, const std::vector<Gridder*>& ggs,
-                       const std::vector<Chunk>& chunks) {
+                       const std::vector<Chunk>& chunks, const std::vector<Gridder*>& psfs,
+                       const std::vector<Gridder*>& pcfs) {
   const size_t n = dgs.size();
   throw_if(n == 0 || ggs.size() != n || chunks.size() != n, YG_ERR_ARG, "instances need a degridder, a gridder and a chunk each");
+  throw_if(!psfs.empty() && psfs.size() != n, YG_ERR_ARG, "one PSF gridder entry per instance");
+  throw_if(!pcfs.empty() && pcfs.size() != n, YG_ERR_ARG, "one preconditioner gridder entry per instance");
   ck(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking), "stream");
   const int nside = (int)std::min<size_t>(8, n);
   side.resize(nside);
@@ -83,6 +91,20 @@ void CycleBatch::build(const std::vector<Gridder*>& dgs, const std::vector<Gridd
     in.dg->prepare_plan_cf(in.obs);
     in.mfs_dg = in.dg->mfs_weights(in.obs);
     in.mfs_gg = in.gg->mfs_weights(in.obs);
+    in.psf = psfs.empty() ? nullptr : psfs[i];
+    in.pcf = pcfs.empty() ? nullptr : pcfs[i];
+    if (in.psf) {
+      throw_if(!in.psf->is_psf(), YG_ERR_STATE, "the PSF gridder must be initialised with dopsf");
+      in.psf->prepare_plan_cf(in.obs);
+      in.psf->bin(in.obs, in.psf_plan);
+      in.mfs_psf = in.psf->mfs_weights(in.obs);
+    }
+    if (in.pcf) {
+      throw_if(!in.pcf->is_pcf(), YG_ERR_STATE, "the preconditioner gridder must be initialised with dopcf");
+      in.pcf->prepare_plan_cf(in.obs);
+      in.pcf->bin(in.obs, in.pcf_plan);
+      in.mfs_pcf = in.pcf->mfs_weights(in.obs);
+    }
   }
   // one uncaptured cycle sizes every buffer and makes the once-per-plan tables
   for (auto& in : inst) {
@@ -90,6 +112,8 @@ void CycleBatch::build(const std::vector<Gridder*>& dgs, const std::vector<Gridd
     ck(cudaStreamSynchronize(main), "warm-up cycle");
     in->dg->check_device_error();
     in->gg->check_device_error();
+    if (in->psf) in->psf->check_device_error();
+    if (in->pcf) in->pcf->check_device_error();
   }
   events.resize(1 + n);
   for (auto& e : events) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -131,6 +155,8 @@ float CycleBatch::run(int cycles) {
   for (auto& in : inst) {
     in->dg->check_device_error();
     in->gg->check_device_error();
+    if (in->psf) in->psf->check_device_error();
+    if (in->pcf) in->pcf->check_device_error();
   }
   return ms;
 }

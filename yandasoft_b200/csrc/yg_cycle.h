@@ -13,11 +13,15 @@ struct CycleBatch {
   struct Instance {
     Gridder* dg = nullptr;     // holds the model grids
     Gridder* gg = nullptr;     // receives the residual
+    Gridder* psf = nullptr;    // PSF gridder (initialised with dopsf), optional
+    Gridder* pcf = nullptr;    // preconditioner-function gridder (dopcf), optional
     Chunk obs, model, resid;   // device chunks sharing uvw, frequencies, flags and noise
     DevBuf model_vis, resid_vis;
-    Plan plan;
+    Plan plan, psf_plan, pcf_plan;
     const float* mfs_dg = nullptr;
     const float* mfs_gg = nullptr;
+    const float* mfs_psf = nullptr;
+    const float* mfs_pcf = nullptr;
   };
   std::vector<std::unique_ptr<Instance>> inst;
   std::vector<cudaStream_t> side;
@@ -30,7 +34,9 @@ struct CycleBatch {
   CycleBatch() = default;
   CycleBatch(const CycleBatch&) = delete;
   ~CycleBatch();
-  void build(const std::vector<Gridder*>& dgs, const std::vector<Gridder*>& ggs, const std::vector<Chunk>& chunks);
+  // psfs / pcfs: empty, or one (possibly null) gridder per instance
+  void build(const std::vector<Gridder*>& dgs, const std::vector<Gridder*>& ggs, const std::vector<Chunk>& chunks,
+             const std::vector<Gridder*>& psfs = {}, const std::vector<Gridder*>& pcfs = {});
   // replays the graph `cycles` times; returns the GPU milliseconds
   float run(int cycles);
 

@@ -419,10 +419,20 @@ void Gridder::sync() {
   cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
 }
 
+// the device error record copied into mapped host memory
+__global__ void k_error_out(const DevError* __restrict__ d, DevError* h) {
+  h->code = d->code;
+  h->where = d->where;
+}
+
 void Gridder::check_error() {
-  DevError h{};
-  cuda_check(cudaMemcpyAsync(&h, err_.p, sizeof(DevError), cudaMemcpyDeviceToHost, stream_), "error readback");
+  cuda_check(err_h_.ensure(sizeof(DevError)), "alloc error mirror");
+  k_error_out<<<1, 1, 0, stream_>>>(err_.as<DevError>(), err_h_.as<DevError>());
+  cuda_check(cudaGetLastError(), "error readback");
   cuda_check(cudaStreamSynchronize(stream_), "kernel execution");
+  DevError h{};
+  h.code = err_h_.as<volatile DevError>()->code;
+  h.where = err_h_.as<volatile DevError>()->where;
   if (h.code != YG_OK) {
     cudaMemsetAsync(err_.p, 0, sizeof(DevError), stream_);
     cudaStreamSynchronize(stream_);
@@ -483,10 +493,12 @@ void Gridder::init_sumw() {
 
 void Gridder::initialise_grid(const Axes& axes, int nx, int ny, int npol, int nchan, bool dopsf, bool dopcf) {
   ensure_device();
-  throw_if(dopcf, YG_ERR_UNSUPPORTED, "preconditioner-function gridding (dopcf) is not supported");
+  throw_if(dopsf && dopcf, YG_ERR_UNSUPPORTED,
+           "a gridder is configured for the PSF or for the preconditioner function, not both at once");
+  throw_if(dopcf && cf_form_ != 0, YG_ERR_UNSUPPORTED, "the preconditioner function uses the tabulated CFs");
   init_axes(axes, nx, ny, npol, nchan);
   psf_ = dopsf;
-  pcf_ = false;
+  pcf_ = dopcf;
   model_empty_ = false;
   const size_t bytes = (size_t)ngrids() * grid_elems() * sizeof(float2);
   cuda_check(grids_.ensure(bytes), "alloc grids");
@@ -547,12 +559,16 @@ void Gridder::upload_chunk(const Chunk& c, Chunk& dc, bool need_vis, bool vis_wr
   dc.flag = (const uint8_t*)up(up_flag_, c.flag, (size_t)n * c.npol);
   dc.feed1 = (const int*)up(up_feed_, c.feed1, (size_t)c.nrow * sizeof(int));
   dc.pointing = c.pointing;  // host-side use only
+  dc.host_freq = c.freq;
   dc.on_device = 1;
 }
 
+// The chunk's frequencies on the host: from the caller's host array when the
+// chunk was staged from one, else read back from the device.
 static std::vector<double> host_freqs(const Chunk& c) {
   std::vector<double> f(c.nchan);
-  if (c.on_device) cuda_check(cudaMemcpy(f.data(), c.freq, c.nchan * sizeof(double), cudaMemcpyDeviceToHost), "freq");
+  if (c.host_freq) std::memcpy(f.data(), c.host_freq, c.nchan * sizeof(double));
+  else if (c.on_device) cuda_check(cudaMemcpy(f.data(), c.freq, c.nchan * sizeof(double), cudaMemcpyDeviceToHost), "freq");
   else std::memcpy(f.data(), c.freq, c.nchan * sizeof(double));
   return f;
 }
@@ -783,7 +799,8 @@ void Gridder::fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, c
   // 16-wide CFs grid with residue rows modulo their real width (exact rows)
   // unless a layout of several slots per thread was asked for
   const int wpad16 = ((2 * smax + 1) + 15) / 16 * 16;
-  a.wy = (wpad16 == 16 && grid_variant() <= 1 && exact_rows_) ? 2 * smax + 1 : 0;
+  a.wy = (wpad16 == 16 && (grid_variant() & 15) <= 1 && exact_rows_) ? 2 * smax + 1 : 0;
+  a.pos_major = (grid_variant() & 32) ? 1 : 0;
   a.ntx = (nx_ + a.tile - 1) / a.tile;
   a.nty = (ny_ + a.tile - 1) / a.tile;
   int mb = 0;
@@ -862,7 +879,7 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
   check_error();
 }
 
-static VisArgs vis_args(const Chunk& dc, const float* mfs, bool psf) {
+static VisArgs vis_args(const Chunk& dc, const float* mfs, bool psf, bool pcf = false) {
   VisArgs v;
   v.vis = dc.vis;
   v.noise = dc.noise;
@@ -874,6 +891,7 @@ static VisArgs vis_args(const Chunk& dc, const float* mfs, bool psf) {
   v.npol = dc.npol;
   v.psf = psf ? 1 : 0;
   v.psf_ok = nullptr;
+  v.pcf = pcf ? 1 : 0;
   return v;
 }
 
@@ -922,6 +940,7 @@ Chunk Gridder::stage_rows(const Chunk& c, long long r0, long long nr, int b, boo
   dc.flag = (const uint8_t*)up2(s.flag, c.flag, 1);
   dc.feed1 = c.feed1 ? (const int*)up(s.feed, c.feed1 + r0, nrows * sizeof(int)) : nullptr;
   dc.pointing = c.pointing ? c.pointing + 2 * r0 : nullptr;
+  dc.host_freq = c.freq;
   dc.on_device = 1;
   if (!piece_up_[b]) cuda_check(cudaEventCreateWithFlags(&piece_up_[b], cudaEventDisableTiming), "event");
   cuda_check(cudaEventRecord(piece_up_[b], cs), "event");
@@ -951,9 +970,9 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
       const long long r1 = (k + 1) * rows;
       staged[b ^ 1] = stage_rows(c, r1, std::min(rows, c.nrow - r1), b ^ 1, true);
     }
-    // the host waits for this piece's upload (binning reads its frequencies
-    // through a synchronous copy); the next piece's upload runs on
-    cuda_check(cudaEventSynchronize(piece_up_[b]), "wait upload");
+    // the gridder's stream waits for this piece's upload; the next piece's
+    // upload runs on (binning takes the frequencies from the caller's host array)
+    cuda_check(cudaStreamWaitEvent(stream_, piece_up_[b], 0), "wait upload");
     Chunk& dc = staged[b];
     init_cf(dc);
     bin(dc, piece_plan_[b]);
@@ -993,18 +1012,25 @@ void Gridder::grid(const Chunk& c) {
   grid_plan(dc, pl);
 }
 
-// MFS weights of the chunk's channels on the device (null without MFS).
+// MFS weights of the chunk's channels on the device (null without MFS); made
+// again only when the frequencies or the MFS order change.
 const float* Gridder::mfs_weights(const Chunk& dc) {
   if (!mfs_) return nullptr;
   const std::vector<double> f = host_freqs(dc);
-  std::vector<float> w(dc.nchan);
+  if (f == mfs_freqs_ && mfs_key_order_ == mfs_order_ && mfs_key_ref_ == mfs_reffreq_ && mfs_d_.p)
+    return mfs_d_.as<float>();
+  mfs_w_.resize(dc.nchan);
   for (int i = 0; i < dc.nchan; ++i) {
     const double ratio = (f[i] - mfs_reffreq_) / mfs_reffreq_;
-    w[i] = mfs_order_ == 0 ? 1.0f : (mfs_order_ == 1 ? (float)ratio : (mfs_order_ == 2 ? (float)(ratio * ratio) : (float)std::pow(ratio, mfs_order_)));
+    mfs_w_[i] = mfs_order_ == 0 ? 1.0f : (mfs_order_ == 1 ? (float)ratio : (mfs_order_ == 2 ? (float)(ratio * ratio) : (float)std::pow(ratio, mfs_order_)));
   }
   cuda_check(mfs_d_.ensure(dc.nchan * sizeof(float)), "alloc");
-  cuda_check(cudaMemcpyAsync(mfs_d_.p, w.data(), dc.nchan * sizeof(float), cudaMemcpyHostToDevice, stream_), "up");
+  // the host vector stays alive in the gridder until the copy has run
+  cuda_check(cudaMemcpyAsync(mfs_d_.p, mfs_w_.data(), dc.nchan * sizeof(float), cudaMemcpyHostToDevice, stream_), "up");
   cuda_check(cudaStreamSynchronize(stream_), "up");
+  mfs_freqs_ = f;
+  mfs_key_order_ = mfs_order_;
+  mfs_key_ref_ = mfs_reffreq_;
   return mfs_d_.as<float>();
 }
 
@@ -1013,8 +1039,10 @@ const float* Gridder::mfs_weights(const Chunk& dc) {
 // part of grid_plan that a CUDA graph records).
 void Gridder::grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0,
                            cudaEvent_t k1) {
-  VisArgs v = vis_args(dc, mfs, psf_);
-  const SumwArgs sw{sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0, nsumw_rows_, nchan_};
+  VisArgs v = vis_args(dc, mfs, psf_, pcf_);
+  // the preconditioner function adds nothing to the sums of weights
+  const SumwArgs sw{pcf_ ? nullptr : sumw_.as<double>(), pl.chanmap.as<int>(), os_, track_per_os_ ? 1 : 0,
+                    nsumw_rows_, nchan_};
   const LearnedCF lcf = learned_view_for(dc, const_cast<Plan&>(pl));
   rc_check(plan_grid(pl, v, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, sw, scratch_, svis_,
                      err_.as<DevError>(), st, k0, k1, grid_variant(), cf_form_ != 0 ? &lcf : nullptr),
@@ -1055,6 +1083,7 @@ void Gridder::grid_plan(const Chunk& dc, const Plan& pl) {
 
 void Gridder::degrid(Chunk& c) {
   throw_if(psf_, YG_ERR_STATE, "the gridder is not supposed to be used for degridding in the PSF mode");
+  throw_if(pcf_, YG_ERR_STATE, "the gridder is not supposed to be used for degridding in the PCF mode");
   if (model_empty_) return;
   throw_if(nx_ == 0 || !grids_.p, YG_ERR_STATE, "initialiseDegrid must be called before degrid");
   if (pipelined(c)) {

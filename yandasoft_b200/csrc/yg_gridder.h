@@ -57,6 +57,7 @@ struct Chunk {
   const int* feed1 = nullptr;
   const double* pointing = nullptr;
   int on_device = 0;
+  const double* host_freq = nullptr;   // the caller's host copy of freq, when there is one
 };
 
 enum class Kind { SphFunc, WProject, WStack, AWProject, WStackWProject };
@@ -105,6 +106,8 @@ class Gridder {
   void customise_for_context(const std::string& context);
   void init_vis_weights_mfs(double reffreq);
   bool is_model_empty() const { return model_empty_; }
+  bool is_psf() const { return psf_; }
+  bool is_pcf() const { return pcf_; }
 
   // inspection helpers
   Kind kind() const { return kind_; }
@@ -250,6 +253,11 @@ class Gridder {
   LearnedCF learned_view() const;
   LearnedCF learned_view_for(const Chunk& dc, Plan& pl);
   DevBuf grids_, sumw_, carry_, err_, chanmap_d_, rowok_d_, corr_d_;
+  HostMapped err_h_;                   // mapped host mirror of err_ for the read-back
+  std::vector<float> mfs_w_;           // host MFS weights of the last upload
+  std::vector<double> mfs_freqs_;      // frequencies they were made for
+  int mfs_key_order_ = -1;
+  double mfs_key_ref_ = 0.0;
   DevBuf up_uvw_, up_delay_, up_freq_, up_vis_, up_noise_, up_flag_, up_feed_;
   DevBuf scratch_, svis_, tmpvals_, cfwork_, img_tmp_, mfs_d_;
   int nsumw_rows_ = 1;

@@ -241,6 +241,7 @@ struct GridKArgs {
   int pps;                   // CF planes (runs) per stage, CFM 0
   int cfplane;               // bytes of one CF plane slot
   int Wy;                    // row modulus of the residues (the plan's)
+  int pos_major;             // records in position-major order, taps read through L2
   LearnedCF lcf;             // the network of the learned CF mode
   const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   DevError* err;
@@ -328,7 +329,7 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
                                             unsigned char* ring, unsigned long long* full,
                                             unsigned long long* empty, int& seg, bool stage_cf = true,
                                             const float4* __restrict__ ext = nullptr, int nterm = 1, int pps = 1,
-                                            int cfplane = 0) {
+                                            int cfplane = 0, bool cut = true) {
   const int lane = threadIdx.x & 31;
   const unsigned fm = 0xffffffffu;
   const unsigned cfcopy = (unsigned)Wp2 * sizeof(float2);
@@ -360,7 +361,8 @@ __device__ __forceinline__ bool seg_produce(const int4 it, const int4* __restric
     load(base + 32, rn, vn, xn);                   // next window in flight
     const int nwin = min(32, it.z - base);
     const int zprev = __shfl_up_sync(fm, r.z, 1);
-    unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || zprev != r.z));
+    // segments start at CF changes (cut), else one segment per window
+    unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || (cut && zprev != r.z)));
     while (heads) {
       // a stage takes up to pps consecutive runs of the window, each CF plane
       // in a slot of its own; with pps > 1 the staged records carry the slot
@@ -497,7 +499,13 @@ __device__ __forceinline__ float2 mlp_tap_exact(const float* __restrict__ ws, co
 // shared memory when a segment changes CF; 3, the continuous learned CF: every
 // tap thread evaluates the network for its own taps of every sample at the
 // sample's exact offsets and w (staged beside its record).
-template <int NPOL, int MAXSLOTS, int RSTEP, int CFM>
+//
+// RACC (row layouts only): each slot keeps the cell it last accumulated into
+// and its running sum in registers, and adds that sum into the shared-memory
+// tile only when a sample moves the slot to another cell of its residue class
+// (and once at the end of the item), so consecutive samples whose footprints
+// cover the slot's cell cost no shared-memory read-modify-write.
+template <int NPOL, int MAXSLOTS, int RSTEP, int CFM, bool RACC = false>
 __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
   constexpr bool CFS = CFM == 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -535,7 +543,8 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
   int nfill = 0;       // producer: stages filled
   if (warp == ncw) {
     if (!seg_produce<NPOL>(it, a.rec, a.svis, a.npol_total, a.pol0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full,
-                           empty, nfill, CFS, CFM == 3 ? a.ext : nullptr, 1, CFS ? a.pps : 1, a.cfplane)) {
+                           empty, nfill, CFS, CFM == 3 ? a.ext : nullptr, 1, CFS ? a.pps : 1, a.cfplane,
+                           CFM != 1)) {
       if (lane == 0) {
         raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
         s_abort = 1;
@@ -569,6 +578,15 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
     const int PgR = Pg * RSTEP, WpR = Wp * RSTEP, PgW = Pg * Wy;
     const int trash = Pg * Pg + threadIdx.x;     // target of slots beyond Wp^2
     int cur_cfi = -1;
+    // register accumulation: the slot's current cell and its running sums
+    int rcell[RACC ? MAXSLOTS : 1];
+    float2 racc[RACC ? MAXSLOTS : 1][NPOL];
+#pragma unroll
+    for (int q = 0; q < (RACC ? MAXSLOTS : 1); ++q) {
+      rcell[q] = trash;
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) racc[q][p] = make_float2(0.f, 0.f);
+    }
     for (int nseg_done = 0;; ++nseg_done) {
       const int stage = nseg_done % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg_done / NST) & 1u)) {
@@ -595,6 +613,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         float4 xe = make_float4(0.f, 0.f, 0.f, 0.f);
         if (CFM == 3) xe = xs[l];
         const int wcf = (r.y >> 20) & 0x7ff;
+        const bool conj = a.v.pcf && r.y < 0;   // preconditioner: conjugate CF on this half of the plane
         float2 vv[NPOL];
 #pragma unroll
         for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
@@ -623,19 +642,44 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
               c = (jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe) : make_float2(0.f, 0.f);
             } else {
               c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
+              if (conj) c.y = -c.y;
             }
-            // every polarisation's cell is loaded before any is stored (they are
-            // distinct cells), so the loads are in flight together
-            float2 g[NPOL];
+            if (RACC) {
+              const int qq = RACC ? q : 0;
+              if (c2 != rcell[qq]) {
+                // the slot moves to another cell: its running sums go to the tile
+                float2 g[NPOL];
 #pragma unroll
-            for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + c2];
+                for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + rcell[qq]];
 #pragma unroll
-            for (int p = 0; p < NPOL; ++p) {
-              g[p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g[p].x));
-              g[p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g[p].y));
+                for (int p = 0; p < NPOL; ++p) {
+                  g[p].x += racc[qq][p].x;
+                  g[p].y += racc[qq][p].y;
+                  racc[qq][p] = make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + rcell[qq]] = g[p];
+                rcell[qq] = c2;
+              }
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) {
+                racc[qq][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, racc[qq][p].x));
+                racc[qq][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, racc[qq][p].y));
+              }
+            } else {
+              // every polarisation's cell is loaded before any is stored (they are
+              // distinct cells), so the loads are in flight together
+              float2 g[NPOL];
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + c2];
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) {
+                g[p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, g[p].x));
+                g[p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, g[p].y));
+              }
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + c2] = g[p];
             }
-#pragma unroll
-            for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + c2] = g[p];
             cell += PgR;
             tap += WpR;
           }
@@ -648,9 +692,10 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
             const int tq = live[q] ? jx + Wp * jy : 0;
-            const float2 c = CFM == 3 ? ((live[q] && jx < wcf && jy < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe)
-                                                                           : make_float2(0.f, 0.f))
-                                      : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
+            float2 c = CFM == 3 ? ((live[q] && jx < wcf && jy < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe)
+                                                                     : make_float2(0.f, 0.f))
+                                : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
+            if (CFM < 2 && conj) c.y = -c.y;
             float2 g[NPOL];
 #pragma unroll
             for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + cell];
@@ -666,6 +711,19 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[stage]);
+    }
+    if (RACC) {
+      // the running sums of the last cells
+#pragma unroll
+      for (int q = 0; q < (RACC ? MAXSLOTS : 1); ++q) {
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          float2 g = acc_s[p * PG2 + rcell[q]];
+          g.x += racc[q][p].x;
+          g.y += racc[q][p].y;
+          acc_s[p * PG2 + rcell[q]] = g;
+        }
+      }
     }
   }
   __syncthreads();
@@ -683,10 +741,13 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
 
 // Per sorted sample, once per plan: the footprint origin cell inside the
 // padded tile, its residues mod W and the CF width, the CF index, the sample id.
+// Bit 31 of the second word marks the half of the uv plane where the
+// preconditioner-function gridder uses the conjugate CF
+// (TableVisGridder.cc:836-841); other passes ignore it.
 __global__ void k_records(const unsigned int* __restrict__ val, const unsigned int* __restrict__ pos,
                           const int* __restrict__ cfi, const unsigned long long* __restrict__ key, long long nvalid,
                           int mbits, int ncf, long long ntiles, int ntx, int tile, int smax, int Wp, int Wy,
-                          const int* __restrict__ cfsize, int4* __restrict__ rec) {
+                          const int* __restrict__ cfsize, int nx, int ny, int4* __restrict__ rec) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
     const unsigned int s = val[i];
     const unsigned int ps = pos[s];
@@ -697,7 +758,11 @@ __global__ void k_records(const unsigned int* __restrict__ val, const unsigned i
     const int tx = (int)(t % ntx), ty = (int)(t / ntx);
     const int px0 = (int)(ps & 0xffffu) - sup - (tx * tile - smax);
     const int py0 = (int)(ps >> 16) - sup - (ty * tile - smax);
-    rec[i] = make_int4(px0 | (py0 << 16), (px0 % Wp) | ((py0 % Wy) << 10) | (w << 20), c, (int)s);
+    const int iuo = (int)(ps & 0xffffu), ivo = (int)(ps >> 16);
+    const bool conj_half = (ivo < ny / 2 && iuo >= nx / 2) || (ivo <= ny / 2 && iuo < nx / 2);
+    rec[i] = make_int4(px0 | (py0 << 16),
+                       (int)((unsigned)((px0 % Wp) | ((py0 % Wy) << 10) | (w << 20)) | (conj_half ? 0x80000000u : 0u)),
+                       c, (int)s);
   }
 }
 
@@ -737,7 +802,11 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
         if (!(wt > 0.f)) good = false;
         wts[p] = wt;
         float2 o;
-        if (v.psf) {
+        if (v.pcf) {
+          // uVis = wt: the preconditioner ignores the MFS weight
+          o.x = __fmul_rn(1.f, wt);
+          o.y = __fmul_rn(0.f, wt);
+        } else if (v.psf) {
           o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
           o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
         } else {
@@ -749,7 +818,7 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
           ri = __fmul_rn(__fmul_rn(ri, wt), m);
           o = make_float2(rr, ri);
         }
-        out[(size_t)i * v.npol + p] = o;
+        if (out) out[(size_t)i * v.npol + p] = o;
       }
       if (!good) raise_error(err, YG_ERR_WEIGHT, s);
       if (sw.sumw && good) {
@@ -1357,6 +1426,34 @@ static int ceil_log2(unsigned long long v) {
     if (e_ != cudaSuccess) return YG_ERR_CUDA;  \
   } while (0)
 
+// Position-major key of sorted sample i: (grid plane and tile, Morton
+// position in the tile, CF index), from its CF-major key (grid plane and tile,
+// CF index, Morton position); the value is i.
+__global__ void k_pos_keys(const unsigned long long* __restrict__ key, long long nvalid, int mbits, int ncf,
+                           unsigned long long* __restrict__ key2, unsigned int* __restrict__ idx) {
+  const unsigned long long mmask = (1ull << mbits) - 1ull;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = key[i];
+    const unsigned long long hi = k >> mbits;
+    const unsigned long long gct = hi / (unsigned long long)ncf, cfi = hi % (unsigned long long)ncf;
+    key2[i] = (((gct << mbits) | (k & mmask)) * (unsigned long long)ncf) + cfi;
+    idx[i] = (unsigned int)i;
+  }
+}
+
+__global__ void k_permute_rec(const int4* __restrict__ rec, const unsigned int* __restrict__ perm, long long n,
+                              int4* __restrict__ out) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+    out[j] = rec[perm[j]];
+}
+
+// out[0] = work items (base of the last tile + its item count), out[1] = on-grid samples
+__global__ void k_plan_counts(const int* __restrict__ last_base, const int* __restrict__ last_n,
+                              const long long* __restrict__ nvalid, long long* out) {
+  out[0] = (long long)*last_base + *last_n;
+  out[1] = *nvalid;
+}
+
 // Bins one chunk: fills plan (sorted ids, tile table, work items).
 int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t st) {
   const long long n = a.nrow * (long long)a.nchan;
@@ -1435,14 +1532,14 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
   if (tmp2 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp2));
   YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(pl.sort_tmp.p, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
-  int last_base = 0, last_n = 0;
-  long long nvalid = 0;
-  YG_CUDA_TRY(cudaMemcpyAsync(&last_base, pl.itembase.as<int>() + (nt - 1), 4, cudaMemcpyDeviceToHost, st));
-  YG_CUDA_TRY(cudaMemcpyAsync(&last_n, pl.nit.as<int>() + (nt - 1), 4, cudaMemcpyDeviceToHost, st));
-  YG_CUDA_TRY(cudaMemcpyAsync(&nvalid, pl.nvalid_d.p, 8, cudaMemcpyDeviceToHost, st));
+  // item count and on-grid samples back to the host through mapped memory
+  YG_CUDA_TRY(pl.info_h.ensure(16));
+  k_plan_counts<<<1, 1, 0, st>>>(pl.itembase.as<int>() + (nt - 1), pl.nit.as<int>() + (nt - 1),
+                                 pl.nvalid_d.as<long long>(), pl.info_h.as<long long>());
+  YG_COUNT_LAUNCH();
   YG_CUDA_TRY(cudaStreamSynchronize(st));
-  pl.nitems = last_base + last_n;
-  pl.nvalid = nvalid;
+  pl.nitems = (int)pl.info_h.as<volatile long long>()[0];
+  pl.nvalid = pl.info_h.as<volatile long long>()[1];
   YG_CUDA_TRY(pl.items.ensure((size_t)std::max(1, pl.nitems) * sizeof(int4)));
   k_fill_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), pl.nit.as<int>(),
                                                   pl.itembase.as<int>(), nt, vmax, pl.items.as<int4>());
@@ -1467,17 +1564,48 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     k_records<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.val.as<unsigned int>(), pl.pos.as<unsigned int>(),
                                                         pl.cfi.as<int>(), pl.key.as<unsigned long long>(), pl.nvalid,
                                                         a.mbits, a.cf.ncf, (long long)a.ntx * a.nty, a.ntx, a.tile,
-                                                        pl.smax, a.cf.wpad, pl.wy, a.cf.size, pl.rec.as<int4>());
+                                                        pl.smax, a.cf.wpad, pl.wy, a.cf.size, a.nx, a.ny,
+                                                        pl.rec.as<int4>());
     YG_COUNT_LAUNCH();
+  }
+  pl.pos_ready = false;
+  if (a.pos_major && pl.nvalid > 0) {
+    // a second order of the same records for gridding: tile first as before
+    // (the work items stay valid), then the position inside the tile, then
+    // the CF index, so consecutive samples of an item mostly cover the same
+    // cells (register accumulation in k_grid)
+    const long long nv = pl.nvalid;
+    YG_CUDA_TRY(pl.key_alt.ensure(nv * 8));
+    YG_CUDA_TRY(pl.pos_key2.ensure(nv * 8));
+    YG_CUDA_TRY(pl.val_alt.ensure(nv * 4));
+    YG_CUDA_TRY(pl.pos_val2.ensure(nv * 4));
+    k_pos_keys<<<grid_dim(nv, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), nv, a.mbits, a.cf.ncf,
+                                                  pl.key_alt.as<unsigned long long>(), pl.val_alt.as<unsigned int>());
+    YG_COUNT_LAUNCH();
+    cub::DoubleBuffer<unsigned long long> kb2(pl.key_alt.as<unsigned long long>(),
+                                              pl.pos_key2.as<unsigned long long>());
+    cub::DoubleBuffer<unsigned int> vb2(pl.val_alt.as<unsigned int>(), pl.pos_val2.as<unsigned int>());
+    size_t tmp4 = 0;
+    YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp4, kb2, vb2, (int)nv, 0, end_bit, st));
+    if (tmp4 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp4));
+    YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(pl.sort_tmp.p, tmp4, kb2, vb2, (int)nv, 0, end_bit, st));
+    YG_CUDA_TRY(pl.rec_pos.ensure((size_t)nv * sizeof(int4)));
+    k_permute_rec<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec.as<int4>(), vb2.Current(), nv, pl.rec_pos.as<int4>());
+    YG_COUNT_LAUNCH();
+    YG_CUDA_TRY(cudaGetLastError());
+    YG_CUDA_TRY(cudaStreamSynchronize(st));
+    pl.pos_key2.release();
+    pl.pos_val2.release();
+    pl.pos_ready = true;
   }
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
 }
 
 
-template <int NPOL, int MAXSLOTS, int RSTEP, int CFM = 0>
+template <int NPOL, int MAXSLOTS, int RSTEP, int CFM = 0, bool RACC = false>
 static cudaError_t launch_grid_ms(const GridKArgs& g, int nitems, int threads, size_t smem, cudaStream_t st) {
-  auto k = k_grid<NPOL, MAXSLOTS, RSTEP, CFM>;
+  auto k = k_grid<NPOL, MAXSLOTS, RSTEP, CFM, RACC>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<nitems, threads + 32, smem, st>>>(g);   // tap warps + the producer warp
   YG_COUNT_LAUNCH();
@@ -1582,8 +1710,34 @@ static cudaError_t launch_grid_np_learned(const GridKArgs& g, int nitems, size_t
 }
 
 template <int NPOL>
-static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, GridShape sh, cudaStream_t st) {
+static cudaError_t launch_grid_np(const GridKArgs& g, int nitems, size_t smem, GridShape sh, cudaStream_t st,
+                                  bool racc = false) {
   const int t = sh.threads;
+  if (g.pos_major) {
+    // position-major records, taps through L2, register accumulation (row layouts only)
+    if (!sh.rstep) return cudaErrorInvalidConfiguration;
+    switch (sh.slots * 1000 + sh.rstep) {
+      case 1016: return launch_grid_ms<NPOL, 1, 16, 1, true>(g, nitems, t, smem, st);
+      case 2008: return launch_grid_ms<NPOL, 2, 8, 1, true>(g, nitems, t, smem, st);
+      case 4008: return launch_grid_ms<NPOL, 4, 8, 1, true>(g, nitems, t, smem, st);
+      case 6008: return launch_grid_ms<NPOL, 6, 8, 1, true>(g, nitems, t, smem, st);
+      case 8008: return launch_grid_ms<NPOL, 8, 8, 1, true>(g, nitems, t, smem, st);
+      default: return cudaErrorInvalidConfiguration;
+    }
+  }
+  if (sh.rstep && racc) {
+    // register accumulation: layouts of at most 8 slots per thread
+    switch (sh.slots * 1000 + sh.rstep) {
+      case 1016: return launch_grid_ms<NPOL, 1, 16, 0, true>(g, nitems, t, smem, st);
+      case 2008: return launch_grid_ms<NPOL, 2, 8, 0, true>(g, nitems, t, smem, st);
+      case 4004: return launch_grid_ms<NPOL, 4, 4, 0, true>(g, nitems, t, smem, st);
+      case 4008: return launch_grid_ms<NPOL, 4, 8, 0, true>(g, nitems, t, smem, st);
+      case 6008: return launch_grid_ms<NPOL, 6, 8, 0, true>(g, nitems, t, smem, st);
+      case 8004: return launch_grid_ms<NPOL, 8, 4, 0, true>(g, nitems, t, smem, st);
+      case 8008: return launch_grid_ms<NPOL, 8, 8, 0, true>(g, nitems, t, smem, st);
+      default: break;   // wider layouts accumulate in shared memory
+    }
+  }
   if (sh.rstep) {
     switch (sh.slots * 1000 + sh.rstep) {
       case 1016: return launch_grid_ms<NPOL, 1, 16>(g, nitems, t, smem, st);
@@ -1692,6 +1846,12 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
               const SumwArgs& sw, DevBuf& scratch, DevBuf& svis, DevError* err, cudaStream_t st, cudaEvent_t ev0,
               cudaEvent_t ev1, int mode, const LearnedCF* lcf) {
   const bool learned = lcf && lcf->w16;
+  // mode bits: 16 register accumulation of the row layouts; 32 the
+  // position-major records with taps read through L2 (and register accumulation)
+  const bool pos = (mode & 32) != 0 && pl.pos_ready && !learned && v.npol <= 4;
+  const bool racc = (mode & 16) != 0 || pos;
+  mode &= 15;
+  if (learned && v.pcf) return YG_ERR_UNSUPPORTED;
   if (pl.nitems == 0) return YG_OK;
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
   const int P = pl.pad;
@@ -1707,13 +1867,28 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
   YG_CUDA_TRY(svis.ensure((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
   if (v.npol > 4) return YG_ERR_UNSUPPORTED;
-  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>(), sw, err);
-  YG_COUNT_LAUNCH();
+  if (pos) {
+    // visibilities in the position-major order; the sums of weights over the
+    // CF-major records, whose runs of equal rows keep the atomics few
+    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec_pos.as<int4>(), pl.nvalid, svis.as<float2>(),
+                                                           SumwArgs{nullptr, sw.chan_map, sw.os, sw.track_per_os,
+                                                                    sw.nrows, sw.nchan_img}, err);
+    YG_COUNT_LAUNCH();
+    if (sw.sumw) {
+      k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, nullptr, sw, err);
+      YG_COUNT_LAUNCH();
+    }
+  } else {
+    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>(), sw,
+                                                           err);
+    YG_COUNT_LAUNCH();
+  }
   GridKArgs g;
   g.Wy = pl.wy;
+  g.pos_major = pos ? 1 : 0;
   g.items = pl.items.as<int4>();
   g.val = pl.val.as<unsigned int>();
-  g.rec = pl.rec.as<int4>();
+  g.rec = pos ? pl.rec_pos.as<int4>() : pl.rec.as<int4>();
   g.svis = svis.as<float2>();
   g.runend = pl.runend.as<int>();
   g.pos = pl.pos.as<unsigned int>();
@@ -1759,8 +1934,8 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     g.stage_bytes = seg_stage_bytes(0, npa + xv);
     smem = tile_b + (size_t)g.nstages * st_n + extra;
   } else {
-    npa = grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
-    cf_global = npa == 0;      // CF planes too wide for the ring: taps from global memory
+    npa = pos ? 0 : grid_pols_per_pass(v.npol, Pg, g.cfbuf, shape.threads);
+    cf_global = npa == 0;      // CF planes too wide for the ring (or position-major records): taps from global memory
     if (cf_global) {
       g.cfbuf = 0;
       npa = grid_pols_per_pass(v.npol, Pg, 0, shape.threads);
@@ -1785,12 +1960,15 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
       continue;
     }
     switch (npa * 2 + (cf_global ? 1 : 0)) {
-      case 2: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st); break;
-      case 4: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st); break;
-      case 8: e = launch_grid_np<4>(g, pl.nitems, smem, shape, st); break;
-      case 3: e = launch_grid_np_global<1>(g, pl.nitems, smem, shape, st); break;
-      case 5: e = launch_grid_np_global<2>(g, pl.nitems, smem, shape, st); break;
-      case 9: e = launch_grid_np_global<4>(g, pl.nitems, smem, shape, st); break;
+      case 2: e = launch_grid_np<1>(g, pl.nitems, smem, shape, st, racc); break;
+      case 4: e = launch_grid_np<2>(g, pl.nitems, smem, shape, st, racc); break;
+      case 8: e = launch_grid_np<4>(g, pl.nitems, smem, shape, st, racc); break;
+      case 3: e = pos ? launch_grid_np<1>(g, pl.nitems, smem, shape, st, true)
+                      : launch_grid_np_global<1>(g, pl.nitems, smem, shape, st); break;
+      case 5: e = pos ? launch_grid_np<2>(g, pl.nitems, smem, shape, st, true)
+                      : launch_grid_np_global<2>(g, pl.nitems, smem, shape, st); break;
+      case 9: e = pos ? launch_grid_np<4>(g, pl.nitems, smem, shape, st, true)
+                      : launch_grid_np_global<4>(g, pl.nitems, smem, shape, st); break;
       default: return YG_ERR_UNSUPPORTED;
     }
     if (e == cudaErrorInvalidConfiguration) return YG_ERR_UNSUPPORTED;
@@ -2024,7 +2202,7 @@ int plan_learned_inputs(Plan& pl, const double* uvw, const double* freq, double 
 // sample's visibility in loop order.
 int plan_grid_carry(Plan& pl, const VisArgs& v, float2* carry, cudaStream_t st) {
   const long long n = pl.nsamples;
-  if (n == 0 || v.psf) return YG_OK;
+  if (n == 0 || v.psf || v.pcf) return YG_OK;
   YG_CUDA_TRY(pl.last.ensure(sizeof(int)));
   YG_CUDA_TRY(cudaMemsetAsync(pl.last.p, 0xff, sizeof(int), st));
   k_last_marked<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 1,

@@ -40,6 +40,32 @@ struct DevBuf {
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Small page-locked host buffer mapped into the device's address space: a
+// kernel writes it and the host reads it after synchronising the stream, so a
+// read-back of a few values never waits in a copy engine's queue behind a
+// large transfer of another stream.
+struct HostMapped {
+  void* p = nullptr;
+  size_t bytes = 0;
+  HostMapped() = default;
+  HostMapped(const HostMapped&) = delete;
+  HostMapped& operator=(const HostMapped&) = delete;
+  ~HostMapped() {
+    if (p) cudaFreeHost(p);
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) { p = nullptr; return e; }
+    bytes = n;
+    return cudaSuccess;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
 // Convolution-function cache in HBM: every CF matrix (odd size, u fastest)
 // packed back to back.
 struct CFView {
@@ -84,6 +110,7 @@ struct BinArgs {
   int ntx, nty;            // tiles per axis
   int mbits;               // bits of the within-tile Morton code
   int wy;                  // row modulus of the residues in the records (0: the padded CF width)
+  int pos_major;           // also build the position-major records (rec_pos)
   unsigned long long invalid_key;  // one past the largest valid key
   CFView cf;
 };
@@ -103,12 +130,16 @@ struct Plan {
   int nchan = 0, npol = 0;
   DevBuf key, key_alt, val, val_alt, pos, cfi, status;
   DevBuf tstart, tend, nit, itembase, items, nvalid_d, sort_tmp;
+  HostMapped info_h;            // read-back of the item count and on-grid samples
   DevBuf order_prev;            // degrid stale-value scan: marks, then loop-order predecessors
   bool prev_ready = false;      // order_prev holds this plan's predecessors
   DevBuf last;                  // grid carry: loop-order index of the last used sample
   DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
   DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
   DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
+  DevBuf rec_pos;               // the same records ordered by tile, then position in the tile, then CF
+  DevBuf pos_key2, pos_val2;    // sort buffers of rec_pos (released after the build)
+  bool pos_ready = false;       // rec_pos is built
   DevBuf ext;                   // continuous learned CF: per sorted sample (ru, rv, w, 0)
   bool ext_ready = false;
   int mbits = 0, ncf = 0;       // sort-key layout
@@ -128,6 +159,8 @@ struct VisArgs {
   int npol;
   int psf;                  // grid the weight instead of the visibility
   const uint8_t* psf_ok;    // nrow representative feed/field mask (PSF), may be null
+  int pcf = 0;              // preconditioner function: grid the weight (no MFS factor) with the
+                            // conjugate CF on one half of the uv plane (TableVisGridder.cc:825-851)
 };
 
 // Sums of weights (rows, npol, image channels), column-major, in double; rows

@@ -1,13 +1,14 @@
 // Degridding that allocates no device memory.
 //
-// Some callers of this library cannot call cudaMalloc: a program that records
-// its imaging loop into a CUDA graph while a stream is being captured (device
-// allocation is not an operation that stream capture allows), or a pipeline
-// that hands the GPU a fixed memory budget at start-up and forbids further
-// allocations (real-time and service deployments).  yg_degrid_noalloc serves
-// them: it degrids a device-resident chunk with the convolution functions and
-// the model grid that the gridder already holds, and keeps every per-call
-// temporary in the statically allocated array below.
+// Some callers of this library cannot call cudaMalloc: an application that
+// hands each GPU a fixed memory budget when it starts and forbids any later
+// allocation, so that a long-running imaging service never fails half way
+// through a major cycle for lack of memory, or a host framework whose own
+// pool allocator owns the device's memory and gives no other code a share of
+// it.  yg_degrid_noalloc serves them: it degrids a device-resident chunk with
+// the convolution functions and the model grid that the gridder already
+// holds, and keeps every per-call temporary in the statically allocated array
+// below.
 //
 // The array is a file-scope __device__ array, so every GPU that loads this
 // library holds its kNATotal bytes until the process exits.  In host code its
@@ -16,7 +17,9 @@
 // current) the first time a call runs on it.  Every call shares the one array
 // and the array keeps the previous call's contents, so everything a call needs
 // zeroed is written before use; calls that overlap on the GPU (two streams, or
-// two host threads) race on it and must be serialised by the caller.
+// two host threads) race on it and must be serialised by the caller.  A call
+// reads the chunk's frequencies back to the host and waits for the gridder's
+// stream before it returns, as yg_degrid does.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -48,7 +51,10 @@ constexpr size_t kNAMarkOff = align256(kNAValsOff + kNAMaxSamples * kNAMaxPol * 
 constexpr size_t kNARowOff = align256(kNAMarkOff + kNAMaxSamples * sizeof(int));
 constexpr size_t kNAChanOff = align256(kNARowOff + kNAMaxSamples);
 constexpr size_t kNAMfsOff = align256(kNAChanOff + kNAMaxChan * sizeof(int));
-constexpr size_t kNATotal = align256(kNAMfsOff + kNAMaxChan * sizeof(float));
+constexpr int kNAScanBlock = 1024;                // elements per block of the max-scan
+constexpr int kNAScanBlocks = (int)(kNAMaxSamples / kNAScanBlock);
+constexpr size_t kNAAggrOff = align256(kNAMfsOff + kNAMaxChan * sizeof(float));
+constexpr size_t kNATotal = align256(kNAAggrOff + kNAScanBlocks * sizeof(int));
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNATotal];
 
@@ -214,8 +220,8 @@ __global__ void k_na_degrid(const int4* __restrict__ meta, VisArgs v, CFView cf,
 }
 
 // marks[o] = o when the sample at loop position o = row * nchan + chan was
-// degridded, else -1; then an inclusive max-scan (one CTA) turns the marks
-// into "last degridded position at or before o".
+// degridded, else -1; an inclusive max-scan over the marks then gives, for
+// every o, the last degridded position at or before o.
 __global__ void k_na_marks(const int4* __restrict__ meta, long long nrow, int nchan, int* __restrict__ marks) {
   const long long n = nrow * (long long)nchan;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
@@ -224,25 +230,54 @@ __global__ void k_na_marks(const int4* __restrict__ meta, long long nrow, int nc
   }
 }
 
-__global__ void __launch_bounds__(1024) k_na_maxscan(int* __restrict__ x, long long n) {
-  __shared__ int part[1024];
-  const long long per = (n + blockDim.x - 1) / blockDim.x;
-  const long long b0 = threadIdx.x * per;
-  const long long b1 = min(n, b0 + per);
-  int m = -1;
-  for (long long i = b0; i < b1; ++i) m = max(m, x[i]);
-  part[threadIdx.x] = m;
-  __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    const int t = threadIdx.x >= off ? part[threadIdx.x - off] : -1;
-    __syncthreads();
-    part[threadIdx.x] = max(part[threadIdx.x], t);
-    __syncthreads();
+// inclusive max over the threads of a 1024-thread block (warp shuffles, then
+// the 32 warp totals by the first warp)
+__device__ __forceinline__ int block_incl_max(int v, int* wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, t);
   }
-  int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : -1;
-  for (long long i = b0; i < b1; ++i) {
-    run = max(run, x[i]);
-    x[i] = run;
+  if (lane == 31) wsum[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    int x = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x = max(x, t);
+    }
+    wsum[lane] = x;
+  }
+  __syncthreads();
+  return warp > 0 ? max(v, wsum[warp - 1]) : v;
+}
+
+// Max-scan in three passes over blocks of kNAScanBlock marks: each block's
+// inclusive scan in place with its total in aggr[b]; one block scans the
+// totals; each element then takes the max with the totals of the blocks before
+// its own.
+__global__ void __launch_bounds__(kNAScanBlock) k_na_scan_blocks(int* __restrict__ x, long long n,
+                                                                  int* __restrict__ aggr) {
+  __shared__ int wsum[32];
+  const long long i = (long long)blockIdx.x * kNAScanBlock + threadIdx.x;
+  const int v = block_incl_max(i < n ? x[i] : -1, wsum);
+  if (i < n) x[i] = v;
+  if (threadIdx.x == kNAScanBlock - 1) aggr[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(kNAScanBlock) k_na_scan_aggr(int* __restrict__ aggr, int nblocks) {
+  __shared__ int wsum[32];
+  const int v = block_incl_max(threadIdx.x < nblocks ? aggr[threadIdx.x] : -1, wsum);
+  if (threadIdx.x < nblocks) aggr[threadIdx.x] = v;
+}
+
+__global__ void k_na_scan_add(int* __restrict__ x, long long n, const int* __restrict__ aggr) {
+  for (long long i = (long long)(blockIdx.x + 1) * kNAScanBlock + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / kNAScanBlock);
+    x[i] = max(x[i], aggr[b - 1]);
   }
 }
 
@@ -289,6 +324,12 @@ long long noalloc_max_samples() { return kNAMaxSamples; }
 
 void Gridder::degrid_noalloc(Chunk& c) {
   na_require(!psf_, YG_ERR_STATE, "the gridder is not supposed to be used for degridding in the PSF mode");
+  // AWProject builds its CFs per chunk (field, beams, channels), which needs
+  // device memory; the learned CF forms run through the plan kernels
+  na_require(kind_ != Kind::AWProject, YG_ERR_UNSUPPORTED,
+             "yg_degrid_noalloc does not take AWProject gridders (their CFs are built per chunk); use yg_degrid");
+  na_require(cf_form_ == 0, YG_ERR_UNSUPPORTED,
+             "yg_degrid_noalloc uses the tabulated CFs only; set the CF form back to 0 or use yg_degrid");
   na_require(c.on_device, YG_ERR_ARG, "yg_degrid_noalloc needs a device-resident chunk (on_device = 1)");
   na_require(nx_ > 0 && grids_.p && device_ready_, YG_ERR_STATE,
              "initialiseDegrid must be called before yg_degrid_noalloc");
@@ -363,7 +404,11 @@ void Gridder::degrid_noalloc(Chunk& c) {
     default: k_na_degrid<4><<<blocks, 256, 0, stream_>>>(meta, v, cf, grids_.as<float2>(), nx_, ny_, nchan_, chanmap, vals); break;
   }
   k_na_marks<<<na_blocks(n), 256, 0, stream_>>>(meta, c.nrow, c.nchan, marks);
-  k_na_maxscan<<<1, 1024, 0, stream_>>>(marks, n);
+  const int nsb = (int)((n + kNAScanBlock - 1) / kNAScanBlock);
+  int* aggr = reinterpret_cast<int*>(base + kNAAggrOff);
+  k_na_scan_blocks<<<nsb, kNAScanBlock, 0, stream_>>>(marks, n, aggr);
+  k_na_scan_aggr<<<1, kNAScanBlock, 0, stream_>>>(aggr, nsb);
+  if (nsb > 1) k_na_scan_add<<<nsb - 1, kNAScanBlock, 0, stream_>>>(marks, n, aggr);
   k_na_writeback<<<na_blocks(n), 256, 0, stream_>>>(meta, marks, vals, carry_.as<float2>(), c.nrow, c.nchan, c.npol, c.vis);
   k_na_carry<<<1, 32, 0, stream_>>>(marks, c.nrow, c.nchan, c.npol, vals, carry_.as<float2>());
   na_cuda(cudaGetLastError(), "yg_degrid_noalloc launch");

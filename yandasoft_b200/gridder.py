@@ -39,6 +39,7 @@ EXPORTS = [
     "yg_set_grid_variant", "yg_degrid_noalloc", "yg_mlp_nparams", "yg_learned_train", "yg_set_cf_form",
     "yg_learned_get_params", "yg_learned_set_params", "yg_mlp_loss_grad", "yg_mlp_eval",
     "yg_cycle_create", "yg_cycle_run", "yg_cycle_info", "yg_cycle_destroy", "yg_autotune", "yg_autotune_reset",
+    "yg_cycle_create_roles",
 ]
 
 
@@ -118,6 +119,7 @@ def load(path: str | None = None):
     L.yg_set_item_size.argtypes = [P, I32]
     L.yg_set_grid_variant.argtypes = [P, I32]
     L.yg_degrid_noalloc.argtypes = [P, ctypes.POINTER(yg_chunk)]
+    L.yg_cycle_create_roles.argtypes = [I32, P, P, ctypes.POINTER(P)]
     L.yg_synchronize.argtypes = [P]
     L.yg_get_stream.argtypes = [P, ctypes.POINTER(P)]
     L.yg_get_kernel_times.argtypes = [P, P]
@@ -439,6 +441,16 @@ class IVisGridder:
             out.append(None if n == 0 else data[offs[i]:offs[i] + n * n].reshape((n, n), order="F"))
         return out
 
+    def cf_bytes(self) -> int:
+        """Bytes of the tabulated CF cache (every matrix, unpadded)."""
+        _, _, ncf = self.support()
+        if ncf == 0:
+            return 0
+        sizes = np.zeros(ncf, dtype=np.int32)
+        offs = np.zeros(ncf, dtype=np.int64)
+        _check(self._lib.yg_get_cf(self.h, sizes.ctypes.data, offs.ctypes.data, None, 0))
+        return int(np.sum(sizes.astype(np.int64) ** 2) * 8)
+
     def cf_offsets(self):
         n = I32()
         _check(self._lib.yg_get_cf_offsets(self.h, None, 0, ctypes.byref(n)))
@@ -481,25 +493,42 @@ class IVisGridder:
         return dict(zip(keys, out.tolist()))
 
 
+class yg_cycle_roles(ctypes.Structure):
+    _fields_ = [("model", P), ("residual", P), ("psf", P), ("pcf", P)]
+
+
 class MajorCycle:
     """degrid -> subtract -> grid for n instances, recorded once as one CUDA
     graph (each instance on a branch of its own) and replayed per cycle.
     degridders[i] holds the model (initialiseDegrid), gridders[i] receives the
     residual (initialiseGrid), accessors[i] are device-resident observed
-    chunks.  See yg_cycle_create."""
+    chunks; psf[i] / pcf[i] (optional, None entries allowed) grid the PSF
+    (initialiseGrid with dopsf) and the preconditioner function (dopcf) from
+    the same buffer.  See yg_cycle_create and yg_cycle_create_roles."""
 
-    def __init__(self, degridders, gridders, accessors):
+    def __init__(self, degridders, gridders, accessors, psf=None, pcf=None):
         self._lib = load()
         n = len(degridders)
         if not (len(gridders) == n == len(accessors)):
             raise AskapError(1, "one degridder, gridder and accessor per instance")
-        self._keep = (list(degridders), list(gridders), list(accessors))
-        dg = (P * n)(*[g.h for g in degridders])
-        gg = (P * n)(*[g.h for g in gridders])
+        psf = list(psf) if psf is not None else [None] * n
+        pcf = list(pcf) if pcf is not None else [None] * n
+        if len(psf) != n or len(pcf) != n:
+            raise AskapError(1, "one PSF and one preconditioner entry per instance")
+        self._keep = (list(degridders), list(gridders), list(accessors), psf, pcf)
         ch = (yg_chunk * n)(*[a.c() for a in accessors])
-        self._arrays = (dg, gg, ch)
         self.h = P()
-        _check(self._lib.yg_cycle_create(n, dg, gg, ch, ctypes.byref(self.h)))
+        if all(g is None for g in psf + pcf):
+            dg = (P * n)(*[g.h for g in degridders])
+            gg = (P * n)(*[g.h for g in gridders])
+            self._arrays = (dg, gg, ch)
+            _check(self._lib.yg_cycle_create(n, dg, gg, ch, ctypes.byref(self.h)))
+        else:
+            roles = (yg_cycle_roles * n)(*[yg_cycle_roles(d.h, g.h, None if s is None else s.h,
+                                                          None if c is None else c.h)
+                                           for d, g, s, c in zip(degridders, gridders, psf, pcf)])
+            self._arrays = (roles, ch)
+            _check(self._lib.yg_cycle_create_roles(n, ctypes.cast(roles, P), ctypes.cast(ch, P), ctypes.byref(self.h)))
 
     def run(self, cycles=1) -> float:
         """Replays the graph `cycles` times; returns the GPU milliseconds."""
