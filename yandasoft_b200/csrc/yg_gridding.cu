@@ -788,8 +788,9 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
     if (i < nvalid) {
       const int4 r = rec[i];
       const long long s = r.w;
-      const long long row = s % v.nrow;
-      const int chan = (int)(s / v.nrow);
+      const unsigned nr32 = (unsigned)v.nrow;       // plans hold fewer than 2^31 samples
+      const int chan = (int)((unsigned)r.w / nr32);
+      const long long row = (long long)((unsigned)r.w - (unsigned)chan * nr32);
       float pr, pi;
       phasor_of(v, row, chan, &pr, &pi);
       const float m = v.mfs ? v.mfs[chan] : 1.f;
@@ -1293,10 +1294,15 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
         if ((lane & ((1 << sh) - 1)) == 0 && (v & 1) == 0) {
           const int p = v >> 1;
           const long long s = r.w;
-          const long long row = s % a.v.nrow;
-          const int chan = (int)(s / a.v.nrow);
-          float pr, pi;
-          phasor_of(a.v, row, chan, &pr, &pi);
+          // row and channel only for the phasor and the MFS weight (sample
+          // ids and row counts of a plan are below 2^31: 32-bit division)
+          float pr = 1.f, pi = 0.f;
+          int chan = 0;
+          if (a.v.delay || a.v.mfs) {
+            const unsigned su = (unsigned)r.w, nr = (unsigned)a.v.nrow;
+            chan = (int)(su / nr);
+            phasor_of(a.v, (long long)(su - (unsigned)chan * nr), chan, &pr, &pi);
+          }
           float cr = cr0, ci = ci0;
           if (a.v.mfs) {
             const float m = a.v.mfs[chan];
