@@ -56,7 +56,7 @@ class _Cfg(ctypes.Structure):
     _fields_ = [("nx", I32), ("ny", I32), ("npol", I32), ("nchan_img", I32), ("ngrids", I32),
                 ("cellu", D), ("cellv", D), ("os", I32), ("ncf", I32),
                 ("cf_size", P), ("cf_off", P), ("cf_data", P), ("noffsets", I32), ("cf_offsets", P),
-                ("forward", I32), ("psf", I32), ("track_per_os", I32), ("nsumw_rows", I32)]
+                ("forward", I32), ("psf", I32), ("track_per_os", I32), ("nsumw_rows", I32), ("pcf", I32)]
 
 
 class _Stats(ctypes.Structure):
@@ -288,9 +288,10 @@ class OracleGridder:
             return self.stacks.nwplanes
         return 1
 
-    def initialise_grid(self, nx, ny, npol, nchan, cell_x, cell_y, freq_axis=None, dopsf=False):
+    def initialise_grid(self, nx, ny, npol, nchan, cell_x, cell_y, freq_axis=None, dopsf=False, dopcf=False):
         self._init_axes(nx, ny, npol, nchan, cell_x, cell_y, freq_axis)
         self.psf = dopsf
+        self.pcf = dopcf
         self.forward = False
         n = nx * ny * npol * nchan
         buf = np.zeros(n * self._ngrids(), dtype=np.complex64)
@@ -412,7 +413,8 @@ class OracleGridder:
                    self.os, len(sizes), _p(sizes), _p(offs), _p(data),
                    0 if offsets is None else len(self.cache.offsets), _p(offsets),
                    int(forward), int(getattr(self, "psf", False) and not forward), int(self.track_per_os),
-                   self.sumw.shape[0] if self.sumw is not None else 1)
+                   self.sumw.shape[0] if self.sumw is not None else 1,
+                   int(getattr(self, "pcf", False) and not forward))
         flag = chunk.flag if chunk.flag is not None else np.zeros(chunk.vis.shape, dtype=bool, order="F")
         flag = np.asfortranarray(flag.astype(np.uint8))
         noise = chunk.noise if chunk.noise is not None else np.ones(chunk.vis.shape, dtype=np.complex64, order="F")
@@ -500,6 +502,7 @@ class OracleGridder:
         nx, ny, npol, nchan = image.shape
         self._init_axes(nx, ny, npol, nchan, cell_x, cell_y, freq_axis)
         self.psf = False
+        self.pcf = False
         self.model_empty = not np.max(np.abs(image)) > 0
         if self.kind in ("WStack", "WStackWProject"):
             st = self._stack_sampling()

@@ -13,7 +13,9 @@ The learned form replaces a tabulated CF cache by a sinusoidal MLP (SIREN):
 y is (real, imaginary) of the tap divided by the CF table's largest |tap|.
 Weights are stored in FP16 and every product is accumulated in FP32: the
 forward and backward passes here use the FP16-rounded weights, and gradients
-are applied to FP32 master weights (Adam).  Nothing of this exists in the
+are applied to FP32 master weights (Adam).  The activations h0, h1, h2 are
+rounded to FP16 (the operands of the kernels' tensor-core layers); the
+rounding passes gradients straight through.  Nothing of this exists in the
 reference: the targets are the reference's tabulated CFs
 (WProjectVisGridder::initConvolutionFunction, restated in cf.py), and the
 parameter layout below is the one the CUDA kernels use.
@@ -87,30 +89,46 @@ def round16(p):
     return np.asarray(p, dtype=np.float32).astype(np.float16).astype(np.float32)
 
 
-def forward(p, X, dtype=np.float64):
-    """y (n, 2) and the pre-activations, with the FP16-rounded weights."""
+def activations(z, round_act=True):
+    """h_k = sin(z_k); with round_act, h0, h1, h2 rounded to FP16, as they
+    enter the tensor-core layers; h3 (input of the FP32 output layer) never."""
+    hs = [np.sin(zk) for zk in z]
+    if round_act:
+        for k in range(NHID):
+            hs[k] = hs[k].astype(np.float16).astype(hs[k].dtype)
+    return hs
+
+
+def forward(p, X, dtype=np.float64, round_act=True):
+    """y (n, 2) and the pre-activations, with the FP16-rounded weights (and
+    FP16-rounded activations h0..h2 unless round_act is false)."""
     d = unpack(round16(p))
     X = np.asarray(X, dtype=dtype)
     z = [OMEGA0 * (X @ d["W0"].astype(dtype) + d["b0"].astype(dtype))]
     h = np.sin(z[0])
+    if round_act:
+        h = h.astype(np.float16).astype(dtype)
     for k in range(1, NHID + 1):
         z.append(h @ d["W%d" % k].astype(dtype) + d["b%d" % k].astype(dtype))
         h = np.sin(z[-1])
+        if round_act and k < NHID:
+            h = h.astype(np.float16).astype(dtype)
     y = h @ d["Wo"].astype(dtype) + d["bo"].astype(dtype)
     return y, z
 
 
-def loss_and_grad(p, X, T, scale=1.0, dtype=np.float64):
-    """L = scale * sum over samples of |y - t|^2 and dL/dp (padding columns 0)."""
+def loss_and_grad(p, X, T, scale=1.0, dtype=np.float64, round_act=True):
+    """L = scale * sum over samples of |y - t|^2 and dL/dp (padding columns 0);
+    the FP16 rounding of the activations passes gradients straight through."""
     d = unpack(round16(p))
     X = np.asarray(X, dtype=dtype)
     T = np.asarray(T, dtype=dtype)
-    y, z = forward(p, X, dtype)
+    y, z = forward(p, X, dtype, round_act)
     r = y - T
     L = scale * float(np.sum(r * r))
     g = np.zeros(NPARAM, dtype=np.float64)
     dy = 2.0 * scale * r
-    hs = [np.sin(zk) for zk in z]
+    hs = activations(z, round_act)
     g[OFF["Wo"]:OFF["Wo"] + H * NOUT] = (hs[-1].T @ dy).ravel()
     g[OFF["bo"]:OFF["bo"] + NOUT] = dy.sum(0)
     dh = dy @ d["Wo"].astype(dtype).T

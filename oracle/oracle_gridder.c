@@ -31,6 +31,7 @@
 #include <stdint.h>
 #include <string.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #define ORC_C 299792458.0
 #define ORC_PI 3.14159265358979323846
@@ -350,6 +351,7 @@ typedef struct {
     int psf;                 /* PSF gridder */
     int track_per_os;        /* gridder.oversampleweight */
     int nsumw_rows;          /* itsSumWeights.shape()(0) */
+    int pcf;                 /* preconditioner-function (PCF) gridder */
 } orc_cfg;
 
 typedef struct {
@@ -387,6 +389,9 @@ int orc_generic(const orc_cfg *cfg, int64_t nrow, int nchan, int npol,
     int64_t i;
     int ch, pol, e;
     float noisev[8][2];
+    /* conjugate CF of the PCF branch: a buffer per thread, reused by every call */
+    static __thread float *conj_cf = NULL;
+    static __thread int conj_cap = 0;
     if (npol != cfg->npol || npol > 8) {
         snprintf(orc_errmsg, sizeof orc_errmsg, "only identity polarisation conversion is restated");
         return ORC_ERR_CINDEX;
@@ -483,7 +488,7 @@ int orc_generic(const orc_cfg *cfg, int64_t nrow, int nchan, int npol,
                         }
                         if (srow >= cfg->nsumw_rows) return ORC_ERR_SUMW;
                         sw = sumw + srow + (int64_t)cfg->nsumw_rows * (pol + (int64_t)cfg->npol * img_chan);
-                        if (!cfg->psf) {
+                        if (!cfg->psf && !cfg->pcf) {
                             /* rVis = phasor * conj(vis) * wt */
                             const float vr = carry[2 * pol], vi = -carry[2 * pol + 1];
                             float rr = ph_re * vr - ph_im * vi;
@@ -494,13 +499,40 @@ int orc_generic(const orc_cfg *cfg, int64_t nrow, int nchan, int npol,
                             st->samples += 1.0;
                             st->taps += (double)((2 * support + 1) * (2 * support + 1));
                             *sw += wt;
-                        } else if (!psf_ok || psf_ok[i]) {
+                        }
+                        if (cfg->psf && (!psf_ok || psf_ok[i])) {
                             float ur = 1.f * wt, ui = 0.f * wt;
                             if (mfs) { ur *= mfs[ch]; ui *= mfs[ch]; }
                             orc_grid_tap(grid, cfg->nx, cf, ur, ui, iuo, ivo, support);
                             st->samples += 1.0;
                             st->taps += (double)((2 * support + 1) * (2 * support + 1));
                             *sw += wt;
+                        }
+                        if (cfg->pcf) {
+                            /* uVis = wt (no MFS weight); the conjugate CF on one
+                             * half of the uv plane, so that the w information
+                             * kept in the imaginary part adds with conjugate
+                             * symmetry; no sum of weights */
+                            const float ur = 1.f * wt, ui = 0.f * wt;
+                            const int w = 2 * support + 1;
+                            if ((ivo < cfg->ny / 2 && iuo >= cfg->nx / 2) || (ivo <= cfg->ny / 2 && iuo < cfg->nx / 2)) {
+                                int k;
+                                if (conj_cap < w * w) {
+                                    free(conj_cf);
+                                    conj_cap = w * w;
+                                    conj_cf = (float *)malloc(sizeof(float) * 2 * (size_t)conj_cap);
+                                    if (!conj_cf) { conj_cap = 0; return ORC_ERR_CINDEX; }
+                                }
+                                for (k = 0; k < w * w; ++k) {
+                                    conj_cf[2 * k] = cf[2 * k];
+                                    conj_cf[2 * k + 1] = -cf[2 * k + 1];
+                                }
+                                orc_grid_tap(grid, cfg->nx, conj_cf, ur, ui, iuo, ivo, support);
+                            } else {
+                                orc_grid_tap(grid, cfg->nx, cf, ur, ui, iuo, ivo, support);
+                            }
+                            st->samples += 1.0;
+                            st->taps += (double)(w * w);
                         }
                     }
                 }

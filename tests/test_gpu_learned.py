@@ -36,13 +36,22 @@ def test_mlp_gradient_matches_oracle(ygmod, oracle_mod):
 
 
 def test_mlp_eval_matches_oracle(ygmod, oracle_mod):
+    """Batch inference (the tensor-core network, 32 inputs per warp) against
+    the restatement.  Both round h0, h1, h2 to FP16; an activation whose FP32
+    and FP64 values fall on the two sides of an FP16 rounding boundary moves
+    by one FP16 ulp (at most 2^-11 of it), which moves the output by about
+    that times the weights behind it: so the bar is 1e-5 of the output scale
+    for the median sample and 3e-3 for the worst of 1000."""
     from oracle import learned as L
     rng = np.random.default_rng(8)
     p = _random_net(5)
     X = rng.uniform(-1, 1, (1000, L.NIN)).astype(np.float32)
     y = ygmod.mlp_eval(p, X)
     yref, _ = L.forward(p, X)
-    assert np.max(np.abs(y - yref)) <= 1e-4 * np.max(np.abs(yref))
+    scale = np.max(np.abs(yref))
+    err = np.abs(y - yref)
+    assert np.median(err) <= 1e-5 * scale, np.median(err) / scale
+    assert err.max() <= 3e-3 * scale, err.max() / scale
 
 
 def _wproject_case():

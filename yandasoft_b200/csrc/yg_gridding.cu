@@ -444,9 +444,9 @@ __device__ __forceinline__ void seg_drain(int nfill, int NST, unsigned long long
 __device__ __forceinline__ void tap_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
 
 // Learned-CF mode: shared memory past the ring's barriers holds the network
-// (FP32 copies of the FP16 weights) and one evaluated CF plane.
+// (its shared-memory image, yg_mlp.cuh) and one evaluated CF plane.
 __host__ __device__ __forceinline__ size_t learned_smem_bytes(int Wp) {
-  return 16 + (size_t)kMlpParamsPadded * sizeof(float) + (size_t)Wp * Wp * sizeof(float2);
+  return 16 + (size_t)kMlpSmemFloats * sizeof(float) + (size_t)Wp * Wp * sizeof(float2);
 }
 
 // The tap warps evaluate CF plane cfi (width w) into `plane` when the segment
@@ -455,7 +455,12 @@ __device__ __forceinline__ void learned_plane(const float* ws, const LearnedCF& 
                                               float2* plane, int nthr, int& cur) {
   if (cfi == cur) return;
   tap_bar(nthr);
-  for (int q = threadIdx.x; q < Wp * Wp; q += nthr) plane[q] = mlp_tap(ws, L, cfi, q % Wp, q / Wp, w);
+  // warp-uniform trip counts: every lane of a warp evaluates the network together
+  for (int q0 = threadIdx.x & ~31; q0 < Wp * Wp; q0 += nthr) {
+    const int q = min(q0 + (int)(threadIdx.x & 31), Wp * Wp - 1);
+    const float2 c = mlp_tap_warp(ws, L, cfi, q % Wp, q / Wp, w);
+    if (q0 + (int)(threadIdx.x & 31) < Wp * Wp) plane[q] = c;
+  }
   tap_bar(nthr);
   cur = cfi;
 }
@@ -463,9 +468,9 @@ __device__ __forceinline__ void learned_plane(const float* ws, const LearnedCF& 
 // Continuous learned CF: tap (jx, jy) of a sample with CF index cfi, width w,
 // at its own fractional offsets fracu/os + ru, fracv/os + rv and its own w
 // (network input xw), instead of the nearest tabulated offset and plane.
+// Zero outside the CF width; every lane of the warp calls it together.
 __device__ __forceinline__ float2 mlp_tap_exact(const float* __restrict__ ws, const LearnedCF& L, int cfi, int jx,
                                                 int jy, int w, const float4& e) {
-  if (jx >= w || jy >= w) return make_float2(0.f, 0.f);
   const int S = (w - 1) / 2;
   const int fu = cfi % L.os, fv = (cfi / L.os) % L.os;
   const float s1 = 1.f / (float)(S + 1);
@@ -475,7 +480,8 @@ __device__ __forceinline__ float2 mlp_tap_exact(const float* __restrict__ ws, co
   x[2] = e.z;
   x[3] = 0.f;
   x[4] = 0.f;
-  const float2 y = mlp_eval(ws, x);
+  const float2 y = mlp_eval_warp(ws, x);
+  if (jx >= w || jy >= w) return make_float2(0.f, 0.f);
   return make_float2(y.x * L.scale, y.y * L.scale);
 }
 
@@ -520,7 +526,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
   unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
   unsigned long long* empty = full + NST;
   float* ws = reinterpret_cast<float*>((reinterpret_cast<size_t>(empty + NST) + 15) & ~(size_t)15);
-  float2* plane = reinterpret_cast<float2*>(ws + kMlpParamsPadded);
+  float2* plane = reinterpret_cast<float2*>(ws + kMlpSmemFloats);
   __shared__ int s_abort;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -605,6 +611,79 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         const int4 r0 = recs[0];
         learned_plane(ws, a.lcf, r0.z, (r0.y >> 20) & 0x7ff, Wp, plane, nthr, cur_cfi);
       }
+      // register accumulation: the slot's running sums go to the tile when a
+      // sample moves the slot to another cell of its residue class
+      auto racc_add = [&](const int qq, const int c2, const float2 c, const float2 (&vv)[NPOL]) {
+        if (c2 != rcell[qq]) {
+          float2 g[NPOL];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + rcell[qq]];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            g[p].x += racc[qq][p].x;
+            g[p].y += racc[qq][p].y;
+            racc[qq][p] = make_float2(0.f, 0.f);
+          }
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + rcell[qq]] = g[p];
+          rcell[qq] = c2;
+        }
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          racc[qq][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, racc[qq][p].x));
+          racc[qq][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, racc[qq][p].y));
+        }
+      };
+      if (CFM == 1 && RACC && RSTEP != 0) {
+        // position-major records (consecutive samples mostly cover the same
+        // cells): the taps come through L2, so the taps of a batch of samples
+        // are loaded first, all in flight together, then accumulated
+        constexpr int PB = MAXSLOTS <= 1 ? 8 : (MAXSLOTS <= 2 ? 4 : 2);
+        if (rowlive) {
+          for (int l0 = 0; l0 < cnt; l0 += PB) {
+            float2 cp[PB][MAXSLOTS];
+#pragma unroll
+            for (int b = 0; b < PB; ++b) {
+              const int4 r = recs[min(l0 + b, cnt - 1)];
+              int jx = rx[0] - (r.y & 1023);
+              jx += (jx < 0) ? Wp : 0;
+              int jy0 = rowoff[0] - ((r.y >> 10) & 1023);
+              jy0 += (jy0 < 0) ? Wy : 0;
+              const int lim = Wy - jy0;
+              const int tap = jx + Wp * jy0;
+              const float2* __restrict__ cfp = a.cf.pad + (size_t)r.z * Wp2;
+#pragma unroll
+              for (int q = 0; q < MAXSLOTS; ++q)
+                cp[b][q] = __ldg(cfp + (RSTEP * q >= lim ? tap + WpR * q - Wp * Wy : tap + WpR * q));
+            }
+#pragma unroll
+            for (int b = 0; b < PB; ++b) {
+              const int l = l0 + b;
+              if (l < cnt) {
+                const int4 r = recs[l];
+                const bool conj = a.v.pcf && r.y < 0;
+                float2 vv[NPOL];
+#pragma unroll
+                for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
+                const int cb = (r.x & 0xffff) + Pg * ((r.x >> 16) & 0xffff);
+                int jx = rx[0] - (r.y & 1023);
+                jx += (jx < 0) ? Wp : 0;
+                int jy0 = rowoff[0] - ((r.y >> 10) & 1023);
+                jy0 += (jy0 < 0) ? Wy : 0;
+                const int lim = Wy - jy0;
+                const int cell = cb + jx + Pg * jy0;
+#pragma unroll
+                for (int q = 0; q < MAXSLOTS; ++q) {
+                  const int c2 = RSTEP * q >= lim ? cell + PgR * q - PgW : cell + PgR * q;
+                  float2 c = cp[b][q];
+                  if (conj) c.y = -c.y;
+                  racc_add(RACC ? q : 0, c2, c, vv);
+                }
+              }
+            }
+          }
+        }
+      } else
       for (int l = 0; l < cnt; ++l) {
         const int4 r = recs[l];
         const float2* __restrict__ cf_s =
@@ -620,6 +699,21 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
         const int cb = px0 + Pg * py0;
         const int mx = r.y & 1023, my = (r.y >> 10) & 1023;
+        // continuous learned CF: the taps of every slot, evaluated by the whole
+        // warp at once (lanes beyond the residue rows take part and drop theirs)
+        float2 ct[CFM == 3 ? MAXSLOTS : 1];
+        if (CFM == 3 && RSTEP) {
+          int jx = rx[0] - mx;
+          jx += (jx < 0) ? Wp : 0;
+          int jy0 = rowoff[0] - my;
+          jy0 += (jy0 < 0) ? Wy : 0;
+          const int lim = Wy - jy0;
+#pragma unroll
+          for (int q = 0; q < (CFM == 3 ? MAXSLOTS : 1); ++q) {
+            const int row = RSTEP * q >= lim ? jy0 + RSTEP * q - Wy : jy0 + RSTEP * q;
+            ct[q] = mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe);
+          }
+        }
         if (RSTEP && rowlive) {
           int jx = rx[0] - mx;
           jx += (jx < 0) ? Wp : 0;
@@ -638,34 +732,13 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             const int t2 = wrap ? tap - Wp * Wy : tap;
             float2 c;
             if (CFM == 3) {
-              const int row = wrap ? jy0 + RSTEP * q - Wy : jy0 + RSTEP * q;
-              c = (jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe) : make_float2(0.f, 0.f);
+              c = ct[CFM == 3 ? q : 0];
             } else {
               c = CFM == 1 ? __ldg(cf_s + t2) : cf_s[t2];
               if (conj) c.y = -c.y;
             }
             if (RACC) {
-              const int qq = RACC ? q : 0;
-              if (c2 != rcell[qq]) {
-                // the slot moves to another cell: its running sums go to the tile
-                float2 g[NPOL];
-#pragma unroll
-                for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + rcell[qq]];
-#pragma unroll
-                for (int p = 0; p < NPOL; ++p) {
-                  g[p].x += racc[qq][p].x;
-                  g[p].y += racc[qq][p].y;
-                  racc[qq][p] = make_float2(0.f, 0.f);
-                }
-#pragma unroll
-                for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + rcell[qq]] = g[p];
-                rcell[qq] = c2;
-              }
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p) {
-                racc[qq][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, racc[qq][p].x));
-                racc[qq][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, racc[qq][p].y));
-              }
+              racc_add(RACC ? q : 0, c2, c, vv);
             } else {
               // every polarisation's cell is loaded before any is stored (they are
               // distinct cells), so the loads are in flight together
@@ -692,9 +765,8 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
             jy += (jy < 0) ? Wp : 0;
             const int cell = live[q] ? cb + jx + Pg * jy : trash;
             const int tq = live[q] ? jx + Wp * jy : 0;
-            float2 c = CFM == 3 ? ((live[q] && jx < wcf && jy < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, jy, wcf, xe)
-                                                                     : make_float2(0.f, 0.f))
-                                : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
+            // (the learned CF modes use the row layouts only)
+            float2 c = CFM >= 2 ? make_float2(0.f, 0.f) : (CFM == 1 ? __ldg(cf_s + tq) : cf_s[tq]);
             if (CFM < 2 && conj) c.y = -c.y;
             float2 g[NPOL];
 #pragma unroll
@@ -1159,7 +1231,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
   unsigned long long* empty = full + NST;
   float* ws = reinterpret_cast<float*>((reinterpret_cast<size_t>(empty + NST) + 15) & ~(size_t)15);
-  float2* plane = reinterpret_cast<float2*>(ws + kMlpParamsPadded);
+  float2* plane = reinterpret_cast<float2*>(ws + kMlpSmemFloats);
   __shared__ int s_abort;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -1247,9 +1319,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
           // taps of the padding hold zeros in the table (read unconditionally,
           // which keeps the four partial sums' loads independent); the
           // network is evaluated only inside the CF width
-          const float2 cv = CFM == 3 ? ((jx < wcf && row < wcf) ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe)
-                                                                 : make_float2(0.f, 0.f))
-                                     : cf_s[tap];
+          const float2 cv = CFM == 3 ? mlp_tap_exact(ws, a.lcf, r.z, jx, row, wcf, xe) : cf_s[tap];
 #pragma unroll
           for (int p = 0; p < NPOL; ++p) {
             const float2 g = g_s[p * PG2 + cell];

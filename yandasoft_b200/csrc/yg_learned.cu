@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_mlp_train(const float* __r
         for (int i = 0; i < kMlpIn; ++i) a = fmaf(W[kOffW0 + i * kMlpH + j], xs[b8 * 8 + i], a);
         a *= kMlpOmega0;
         zo[b8 * kMlpHP + j] = a;
-        ho[b8 * kMlpHP + j] = sinf(a);
+        ho[b8 * kMlpHP + j] = __half2float(__float2half_rn(sinf(a)));   // FP16 operand of layer 1
       }
     }
     __syncthreads();
@@ -161,7 +161,9 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_mlp_train(const float* __r
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         zo[b8 * kMlpHP + g8 * 8 + q] = a[q];
-        ho[b8 * kMlpHP + g8 * 8 + q] = sinf(a[q]);
+        // h1, h2 are the FP16 operands of the next tensor-core layer; h3 stays FP32
+        const float hv = sinf(a[q]);
+        ho[b8 * kMlpHP + g8 * 8 + q] = k < kMlpHid ? __half2float(__float2half_rn(hv)) : hv;
       }
       __syncthreads();
     }
@@ -321,18 +323,24 @@ __global__ void k_mlp_round16(const float* __restrict__ p, __half* __restrict__ 
     w16[i] = __float2half_rn(p[i]);
 }
 
+// The network over a batch of inputs, 32 per warp on the tensor cores.
 __global__ void __launch_bounds__(128) k_mlp_eval(const __half* __restrict__ w16, const float* __restrict__ X,
                                                   long long n, float* __restrict__ Y) {
   extern __shared__ __align__(16) float ws[];
   mlp_load_smem(w16, ws, threadIdx.x, blockDim.x);
   __syncthreads();
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += stride) {
+    const long long i = i0 + (threadIdx.x & 31);
+    const long long ic = i < n ? i : n - 1;
     float x[kMlpIn];
 #pragma unroll
-    for (int c = 0; c < kMlpIn; ++c) x[c] = X[i * kMlpIn + c];
-    const float2 y = mlp_eval(ws, x);
-    Y[2 * i] = y.x;
-    Y[2 * i + 1] = y.y;
+    for (int c = 0; c < kMlpIn; ++c) x[c] = X[ic * kMlpIn + c];
+    const float2 y = mlp_eval_warp(ws, x);
+    if (i < n) {
+      Y[2 * i] = y.x;
+      Y[2 * i + 1] = y.y;
+    }
   }
 }
 
@@ -365,7 +373,7 @@ int mlp_grad(const float* p_d, const float* X_d, const float* T_d, long long n, 
 
 int mlp_eval_batch(const __half* w16_d, const float* X_d, long long n, float* Y_d, cudaStream_t st) {
   if (n <= 0) return YG_OK;
-  const size_t smem = (size_t)kMlpParamsPadded * sizeof(float);
+  const size_t smem = (size_t)kMlpSmemFloats * sizeof(float);
   ML_TRY(cudaFuncSetAttribute(k_mlp_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int blocks = (int)std::min<long long>((n + 127) / 128, 148 * 8);
   k_mlp_eval<<<blocks, 128, smem, st>>>(w16_d, X_d, n, Y_d);
