@@ -230,7 +230,8 @@ class Accessor:
         """The visibility cube as a (nrow, nchan, npol) complex64 Fortran array."""
         if not self.on_device:
             return self.vis
-        flat = self.vis.detach().cpu().numpy().view(np.complex64)
+        # the tensor's memory, in its own (contiguous) order, is the column-major cube
+        flat = self.vis.detach().contiguous().cpu().numpy().view(np.complex64).reshape(-1)
         return flat.reshape((self.nrow, self.nchan, self.npol), order="F")
 
     def c(self):
