@@ -171,7 +171,9 @@ int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
  * keeps each thread's running tap sums in registers while consecutive
  * samples cover the same cell (layouts of at most 8 rows per thread); adding
  * 32 as well orders each tile's samples by position before CF for gridding
- * (plans made afterwards keep both orders) and reads the taps through L2. */
+ * (plans made afterwards keep both orders) and reads the taps through L2;
+ * adding 64 orders them by CF plane, then position, then oversampling offset
+ * and stages each plane's offsets in shared memory once (16-wide CFs). */
 int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */

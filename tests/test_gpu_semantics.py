@@ -411,3 +411,36 @@ def test_preconditioner_function_gridder(ygmod, oracle_mod, kind, npol):
     gd = gg.clone()
     with pytest.raises(Exception):
         gd.degrid(Accessor(ds.uvw, ds.freq, np.zeros_like(ds.vis)))
+
+
+@pytest.mark.parametrize("variant,pcf", [(65, False), (65, True), (66, False), (67, True), (49, False), (17, False)])
+def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
+    """The k_grid variants the autotuner may pick, each against the oracle on
+    flagged, weighted, phase-rotated data with 4 polarisations: 65 (records in
+    plane-major order, each CF plane's oversampling offsets staged in shared
+    memory, register accumulation; 7-wide CFs in 16-wide rows), 49
+    (position-major records, taps through L2) and 17 (register accumulation
+    over the CF-major records).  Grids 1e-5, sums of weights exact; the
+    preconditioner's conjugate half through the plane-major kernel."""
+    from yandasoft_b200.gridder import Accessor, Axes
+    import oracle
+    ds = _data(npol=4, nchan=4, seed=61, duration=300.0)
+    flag, noise, delay = _flags_noise_delay(ds, seed=13)
+    wmax = _wmax(ds.uvw, ds.freq)
+    nx, cell = 1024, 6.0 * ARCSEC
+    params = {"wmax": wmax, "nwstacks": 9, "nwplanes": 9, "oversample": 8, "maxsupport": 512}
+    og, gg = make_pair("WStackWProject", params, oracle_kw={"nwstacks": 9})
+    gg.set_grid_variant(variant)
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, 4, 1), dopcf=pcf)
+    acc = Accessor(ds.uvw, ds.freq, ds.vis, noise=noise, flag=flag, delay=delay).to_device()
+    plan = gg.plan(acc)
+    gg.grid_plan(plan, acc)
+    og.initialise_grid(nx, nx, 4, 1, cell, cell, dopcf=pcf)
+    og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=noise, flag=flag, delay=delay))
+    assert gg.support()[0] == og.cache.support <= 7
+    gpu = np.stack(gg.grids())
+    ref = np.stack(og.grids)
+    assert np.abs(ref).max() > 0
+    err = rel_l2(gpu, ref)
+    assert err < TOL, err
+    assert np.array_equal(gg.sum_weights(), og.sumw)

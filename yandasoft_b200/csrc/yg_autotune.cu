@@ -71,9 +71,12 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   std::vector<int> vmaxes = {def_vmax};
   for (int v : {def_vmax / 4, def_vmax * 4})
     if (v >= 128 && v <= (1 << 20)) vmaxes.push_back(v);
-  // thread layouts: the default, half the threads; then the default with
-  // register accumulation, and with position-major records (taps through L2)
-  const std::vector<int> variants = {1, 2, 17, 49};
+  // thread layouts: the default; the plane-major records with staged CF
+  // planes and one, two or four residue rows per thread; half the threads
+  // (register accumulation over the CF-major records, 16, and position-major
+  // records with taps through L2, 32, measured slower on the benchmark
+  // workloads: not tried)
+  const std::vector<int> variants = {1, 65, 66, 67, 2};
   const int save_tile = tile_override_, save_vmax = vmax_, save_mode = grid_mode_;
   Chunk scratch_chunk = dc;
   DevBuf model;

@@ -799,8 +799,9 @@ void Gridder::fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, c
   // 16-wide CFs grid with residue rows modulo their real width (exact rows)
   // unless a layout of several slots per thread was asked for
   const int wpad16 = ((2 * smax + 1) + 15) / 16 * 16;
-  a.wy = (wpad16 == 16 && (grid_variant() & 15) <= 1 && exact_rows_) ? 2 * smax + 1 : 0;
-  a.pos_major = (grid_variant() & 32) ? 1 : 0;
+  // (the plane-major kernel keeps exact rows with every layout)
+  a.wy = (wpad16 == 16 && ((grid_variant() & 15) <= 1 || (grid_variant() & 64)) && exact_rows_) ? 2 * smax + 1 : 0;
+  a.pos_major = (grid_variant() & 64) ? 2 : ((grid_variant() & 32) ? 1 : 0);
   a.ntx = (nx_ + a.tile - 1) / a.tile;
   a.nty = (ny_ + a.tile - 1) / a.tile;
   int mb = 0;

@@ -315,6 +315,10 @@ __host__ __device__ __forceinline__ int seg_stage_bytes(int cfbuf, int npol) {
 // segments ahead; large ones carry many taps per segment, so two suffice.
 static int min_stages_two_ctas(size_t stage) { return stage >= 8192 ? 2 : 4; }
 
+// dynamic shared memory per CTA with three CTAs per SM (228 kB per SM, 1 kB
+// reserved per CTA, a little kept for the static variables)
+constexpr size_t kSmem3Ctas = 75 * 1024 - 128;
+
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -797,6 +801,240 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
         }
       }
     }
+  }
+  __syncthreads();
+  if (s_abort) {
+    if (warp == ncw && lane == 0) seg_drain(nfill, NST, full);
+    return;
+  }
+  const int P = a.P, P2 = P * P;
+  float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
+  for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
+    const int p = i / P2, c = i % P2;
+    out[i] = acc_s[p * PG2 + (c % P) + Pg * (c / P)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_grid_pl: gridding of one work item whose samples are in plane-major order
+// (CF plane, then position in the tile, then oversampling offset), for
+// 16-wide CFs with exact residue rows (thread t owns x residue t mod 16 and
+// the y residues t / 16 + RY q < Wy of its SL slots, RY = ceil(Wy / SL)).  The producer warp stages records and
+// visibilities in segments of up to 32 samples of one CF plane and, when a
+// segment starts a new plane, brings every oversampling offset of that plane
+// (rows 0..Wy-1 of each padded CF, os^2 bulk copies) into one plane buffer,
+// after all earlier segments are consumed.  Consecutive samples of a plane
+// mostly cover the same cells, so each thread keeps its cell's running sums
+// in registers and adds them into the shared-memory tile only when a sample
+// moves it to another cell of its residue class (GridKernel::grid's sums,
+// GridKernel.cc:57-97, in another order).
+// ---------------------------------------------------------------------------
+template <int NPOL, int SL>
+__global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nthr = blockDim.x - 32;
+  const int ncw = nthr / 32;
+  const int Pg = a.Pg, Wy = a.Wy, os2 = a.pps;       // pps carries os^2 in this kernel
+  const int PG2 = Pg * Pg + nthr;
+  float2* acc_s = reinterpret_cast<float2*>(smem_raw);
+  size_t off = ((size_t)NPOL * PG2 * sizeof(float2) + 127) & ~(size_t)127;
+  float2* planebuf = reinterpret_cast<float2*>(smem_raw + off);
+  const int prow = Wy * 16;                           // float2 per oversampling offset
+  off += ((size_t)os2 * prow * sizeof(float2) + 127) & ~(size_t)127;
+  unsigned char* ring = smem_raw + off;
+  const int SB = a.stage_bytes, NST = a.nstages;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
+  unsigned long long* empty = full + NST;
+  __shared__ int s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int4 it = a.items[blockIdx.x];
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], ncw);
+    }
+    mbar_fence_init();
+  }
+  for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) acc_s[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  int nfill = 0;
+  if (warp == ncw) {
+    // ---- producer
+    const unsigned fm = 0xffffffffu;
+    const unsigned rowbytes = (unsigned)prow * sizeof(float2);
+    int seg = 0, cur_plane = -1;
+    bool ok = true;
+    auto load = [&](int base, int4& r, float2 (&v)[NPOL]) {
+      const int i = base + lane;
+      if (i < it.z) {
+        r = a.rec[i];
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) v[p] = a.svis[(size_t)i * a.npol_total + a.pol0 + p];
+      } else {
+        r = make_int4(0, 0, -1, -1);
+      }
+    };
+    auto acquire = [&](int stage) -> bool {
+      bool okw = true;
+      if (seg >= NST && lane == 0) okw = mbar_wait(&empty[stage], (unsigned)((seg / NST) - 1) & 1u);
+      return __shfl_sync(fm, okw ? 1 : 0, 0) != 0;
+    };
+    int4 r;
+    float2 v[NPOL];
+    load(it.y, r, v);
+    for (int base = it.y; base < it.z && ok; base += 32) {
+      int4 rn;
+      float2 vn[NPOL];
+      load(base + 32, rn, vn);
+      const int nwin = min(32, it.z - base);
+      const int pl = r.z >= 0 ? r.z / os2 : -1;
+      const int plprev = __shfl_up_sync(fm, pl, 1);
+      unsigned heads = __ballot_sync(fm, lane < nwin && (lane == 0 || plprev != pl));
+      while (heads) {
+        const int h = __ffs(heads) - 1;
+        const unsigned rest = heads & (heads - 1);
+        const int h2 = rest ? __ffs(rest) - 1 : nwin;
+        heads = rest;
+        const int stage = seg % NST;
+        if (!acquire(stage)) { ok = false; break; }
+        unsigned char* sp = ring + (size_t)stage * SB;
+        if (lane >= h && lane < h2) {
+          // the sample's decode, done once here for every tap thread: footprint
+          // origin cell, residues (and the preconditioner's conjugate flag),
+          // offset of its oversampling plane in the plane buffer
+          const int cb = (r.x & 0xffff) + Pg * ((r.x >> 16) & 0xffff);
+          const int res = (r.y & 1023) | (((r.y >> 10) & 1023) << 10) | (r.y & (int)0x80000000);
+          reinterpret_cast<int4*>(sp)[lane - h] = make_int4(cb, res, (r.z % os2) * prow, 0);
+          float2* vs = reinterpret_cast<float2*>(sp + kSeg * 16);
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) vs[(lane - h) * NPOL + p] = v[p];
+        }
+        const int plane = __shfl_sync(fm, pl, h);
+        if (lane == 0) {
+          int* hdr = reinterpret_cast<int*>(sp + SB - 16);
+          hdr[0] = h2 - h;
+        }
+        __syncwarp();
+        if (plane != cur_plane) {
+          // the plane buffer is free once every earlier segment is consumed
+          bool okp = true;
+          if (lane == 0) {
+            if (seg >= 1) okp = mbar_wait(&empty[(seg - 1) % NST], (unsigned)((seg - 1) / NST) & 1u);
+            if (okp) {
+              fence_proxy_async_smem();
+              mbar_expect_tx(&full[stage], (unsigned)os2 * rowbytes);
+              for (int f = 0; f < os2; ++f)
+                bulk_g2s(planebuf + (size_t)f * prow, a.cf.pad + ((size_t)plane * os2 + f) * 256, rowbytes,
+                         &full[stage]);
+            }
+          }
+          if (!__shfl_sync(fm, okp ? 1 : 0, 0)) { ok = false; break; }
+          cur_plane = plane;
+        } else if (lane == 0) {
+          mbar_arrive(&full[stage]);
+        }
+        ++seg;
+      }
+      r = rn;
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) v[p] = vn[p];
+    }
+    if (ok) {
+      const int stage = seg % NST;
+      if (acquire(stage)) {
+        if (lane == 0) {
+          reinterpret_cast<int*>(ring + (size_t)stage * SB + SB - 16)[0] = -1;
+          mbar_arrive(&full[stage]);
+        }
+        ++seg;
+      } else {
+        ok = false;
+      }
+    }
+    nfill = seg;
+    if (!ok && lane == 0) {
+      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+      s_abort = 1;
+    }
+  } else {
+    // ---- tap warps: thread t owns x residue t mod 16 and the y residues
+    // t / 16 + RY q, q < SL (RY = ceil(Wy / SL))
+    const int RY = (Wy + SL - 1) / SL;
+    const int rx = threadIdx.x & 15, ry0 = threadIdx.x >> 4;
+    int rcell[SL];
+    float2 racc[SL][NPOL];
+#pragma unroll
+    for (int q = 0; q < SL; ++q) {
+      rcell[q] = Pg * Pg + threadIdx.x;          // this thread's trash cell until the first sample
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) racc[q][p] = make_float2(0.f, 0.f);
+    }
+    const bool live = ry0 < RY;
+    for (int nseg = 0;; ++nseg) {
+      const int stage = nseg % NST;
+      if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+        break;
+      }
+      const unsigned char* sp = ring + (size_t)stage * SB;
+      const int cnt = *reinterpret_cast<const volatile int*>(sp + SB - 16);
+      if (cnt < 0) break;
+      const int4* recs = reinterpret_cast<const int4*>(sp);
+      const float2* vs = reinterpret_cast<const float2*>(sp + kSeg * 16);
+      if (live) {
+        for (int l = 0; l < cnt; ++l) {
+          const int4 r = recs[l];
+          const int jx = (rx - (r.y & 1023)) & 15;
+          const int my = (r.y >> 10) & 1023;
+          const bool conj = a.v.pcf && r.y < 0;
+          float2 vv[NPOL];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
+#pragma unroll
+          for (int q = 0; q < SL; ++q) {
+            const int ry = ry0 + RY * q;
+            if (SL > 1 && ry >= Wy) continue;
+            int jy = ry - my;
+            jy += (jy < 0) ? Wy : 0;
+            float2 c = planebuf[r.z + jy * 16 + jx];
+            if (conj) c.y = -c.y;
+            const int cell = r.x + jx + Pg * jy;
+            if (cell != rcell[q]) {
+              float2 g[NPOL];
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + rcell[q]];
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) {
+                g[p].x += racc[q][p].x;
+                g[p].y += racc[q][p].y;
+                racc[q][p] = make_float2(0.f, 0.f);
+              }
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + rcell[q]] = g[p];
+              rcell[q] = cell;
+            }
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+              racc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, racc[q][p].x));
+              racc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, racc[q][p].y));
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[stage]);
+    }
+#pragma unroll
+    for (int q = 0; q < SL; ++q)
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float2 g = acc_s[p * PG2 + rcell[q]];
+        g.x += racc[q][p].x;
+        g.y += racc[q][p].y;
+        acc_s[p * PG2 + rcell[q]] = g;
+      }
   }
   __syncthreads();
   if (s_abort) {
@@ -1405,6 +1643,8 @@ size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf, int nst) {
 int degrid_t_stages(int npol, int Pg, int cfbuf) {
   const size_t tile = degrid_t_tile_bytes(npol, Pg);
   const size_t stage = (size_t)seg_stage_bytes(cfbuf, 0) + 16;
+  // three CTAs per SM when a stage per tap warp fits beside the tile (small tiles)
+  if (tile + 8 * stage <= kSmem3Ctas) return (int)std::min<size_t>(16, (kSmem3Ctas - tile) / stage);
   if (tile + min_stages_two_ctas(stage) * stage <= 113 * 1024)
     return (int)std::min<size_t>(16, (113 * 1024 - tile) / stage);
   if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(16, (227 * 1024 - tile) / stage);
@@ -1505,14 +1745,22 @@ static int ceil_log2(unsigned long long v) {
 // Position-major key of sorted sample i: (grid plane and tile, Morton
 // position in the tile, CF index), from its CF-major key (grid plane and tile,
 // CF index, Morton position); the value is i.
+// mode 2, plane-major: (grid plane and tile, CF plane = CF index / os^2,
+// Morton position, oversampling offset = CF index mod os^2).
 __global__ void k_pos_keys(const unsigned long long* __restrict__ key, long long nvalid, int mbits, int ncf,
-                           unsigned long long* __restrict__ key2, unsigned int* __restrict__ idx) {
+                           int mode, int os2, unsigned long long* __restrict__ key2, unsigned int* __restrict__ idx) {
   const unsigned long long mmask = (1ull << mbits) - 1ull;
+  const unsigned long long ncp = (unsigned long long)(ncf / os2);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
     const unsigned long long k = key[i];
     const unsigned long long hi = k >> mbits;
     const unsigned long long gct = hi / (unsigned long long)ncf, cfi = hi % (unsigned long long)ncf;
-    key2[i] = (((gct << mbits) | (k & mmask)) * (unsigned long long)ncf) + cfi;
+    if (mode == 2) {
+      const unsigned long long cp = cfi / (unsigned long long)os2, fr = cfi % (unsigned long long)os2;
+      key2[i] = (((((gct * ncp + cp) << mbits) | (k & mmask)) * (unsigned long long)os2) + fr);
+    } else {
+      key2[i] = (((gct << mbits) | (k & mmask)) * (unsigned long long)ncf) + cfi;
+    }
     idx[i] = (unsigned int)i;
   }
 }
@@ -1656,7 +1904,8 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     YG_CUDA_TRY(pl.val_alt.ensure(nv * 4));
     YG_CUDA_TRY(pl.pos_val2.ensure(nv * 4));
     k_pos_keys<<<grid_dim(nv, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), nv, a.mbits, a.cf.ncf,
-                                                  pl.key_alt.as<unsigned long long>(), pl.val_alt.as<unsigned int>());
+                                                  a.pos_major, a.os * a.os, pl.key_alt.as<unsigned long long>(),
+                                                  pl.val_alt.as<unsigned int>());
     YG_COUNT_LAUNCH();
     cub::DoubleBuffer<unsigned long long> kb2(pl.key_alt.as<unsigned long long>(),
                                               pl.pos_key2.as<unsigned long long>());
@@ -1673,6 +1922,8 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     pl.pos_key2.release();
     pl.pos_val2.release();
     pl.pos_ready = true;
+    pl.pos_mode = a.pos_major;
+    pl.os2 = a.os * a.os;
   }
   YG_CUDA_TRY(cudaGetLastError());
   return YG_OK;
@@ -1871,6 +2122,9 @@ size_t grid_smem_bytes(int npol, int Pg, int cfbuf, int nthr, int nst) {
 int grid_stages(int npol, int Pg, int cfbuf, int nthr) {
   const size_t tile = grid_tile_bytes(npol, Pg, nthr);
   const size_t stage = (size_t)seg_stage_bytes(cfbuf, npol) + 16;
+  // three CTAs per SM when the tile is small enough to leave room for the stages
+  if (tile + std::max(3, min_stages_two_ctas(stage)) * stage <= kSmem3Ctas)
+    return (int)std::min<size_t>(8, (kSmem3Ctas - tile) / stage);
   if (tile + min_stages_two_ctas(stage) * stage <= 113 * 1024)
     return (int)std::min<size_t>(8, (113 * 1024 - tile) / stage);
   if (tile + 2 * stage <= 227 * 1024) return (int)std::min<size_t>(8, (227 * 1024 - tile) / stage);
@@ -1924,7 +2178,11 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   const bool learned = lcf && lcf->w16;
   // mode bits: 16 register accumulation of the row layouts; 32 the
   // position-major records with taps read through L2 (and register accumulation)
-  const bool pos = (mode & 32) != 0 && pl.pos_ready && !learned && v.npol <= 4;
+  // mode 64: the plane-major records with each CF plane's offsets staged in
+  // shared memory (k_grid_pl: 16-wide CFs in exact residue rows)
+  const bool planes = (mode & 64) != 0 && pl.pos_ready && pl.pos_mode == 2 && !learned && cf.wpad == 16 &&
+                      pl.wy > 0 && pl.wy <= 16 && !cf.varsup && v.npol <= 4;
+  const bool pos = !planes && (mode & 32) != 0 && pl.pos_ready && pl.pos_mode == 1 && !learned && v.npol <= 4;
   const bool racc = (mode & 16) != 0 || pos;
   mode &= 15;
   if (learned && v.pcf) return YG_ERR_UNSUPPORTED;
@@ -1935,7 +2193,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   GridShape shape = learned ? grid_shape_learned(cf.wpad) : grid_shape_variant(cf.wpad, mode);
   if (pl.wy != cf.wpad) {
     // exact rows: thread t owns x residue t mod 16 and y residue t / 16 < wy
-    if (cf.wpad != 16 || pl.wy > 16 || (!learned && mode > 1)) return YG_ERR_UNSUPPORTED;
+    if (cf.wpad != 16 || pl.wy > 16 || (!learned && mode > 1 && !planes)) return YG_ERR_UNSUPPORTED;
     shape = GridShape{(16 * pl.wy + 31) / 32 * 32, 1, 16};
   }
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
@@ -1955,8 +2213,10 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
       YG_COUNT_LAUNCH();
     }
   } else {
-    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, svis.as<float2>(), sw,
-                                                           err);
+    // plane-major records keep the runs of equal sum-of-weights rows long
+    // (one CF plane after another in each tile): one pass does both
+    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, planes ? pl.rec_pos.as<int4>() : pl.rec.as<int4>(),
+                                                           pl.nvalid, svis.as<float2>(), sw, err);
     YG_COUNT_LAUNCH();
   }
   GridKArgs g;
@@ -2021,6 +2281,52 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     g.stage_bytes = seg_stage_bytes(g.cfbuf, npa);
     smem = grid_smem_bytes(npa, Pg, g.cfbuf, shape.threads, g.nstages);
   }
+  if (planes) {
+    // k_grid_pl: tile + one plane of every oversampling offset + the ring
+    const int os2 = pl.os2;
+    // layout 1: one residue row per thread; 2 and 3: two and four rows
+    const int sl = mode == 3 ? 4 : (mode == 2 ? 2 : 1);
+    const int nthr_pl = (16 * ((pl.wy + sl - 1) / sl) + 31) / 32 * 32;
+    const size_t plane_b = ((size_t)os2 * pl.wy * 16 * sizeof(float2) + 127) & ~(size_t)127;
+    g.rec = pl.rec_pos.as<int4>();
+    g.pps = os2;
+    g.cfbuf = 0;
+    npa = 0;
+    for (int c : {4, 2, 1}) {
+      if (c > v.npol || v.npol % c) continue;
+      const size_t tile_b = ((size_t)c * ((size_t)Pg * Pg + nthr_pl) * sizeof(float2) + 127) & ~(size_t)127;
+      const size_t stage = (size_t)seg_stage_bytes(0, c) + 16;
+      if (tile_b + plane_b + 2 * stage <= 227 * 1024) {
+        npa = c;
+        g.nstages = (int)std::min<size_t>(8, (227 * 1024 - tile_b - plane_b) / stage);
+        g.stage_bytes = seg_stage_bytes(0, c);
+        smem = tile_b + plane_b + (size_t)g.nstages * stage;
+        break;
+      }
+    }
+    if (npa == 0) return YG_ERR_UNSUPPORTED;
+    if (ev0) cudaEventRecord(ev0, st);
+    for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
+      g.pol0 = pol0;
+      auto launch = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<pl.nitems, nthr_pl + 32, smem, st>>>(g);
+        YG_COUNT_LAUNCH();
+      };
+      switch (npa * 10 + sl) {
+        case 11: launch(k_grid_pl<1, 1>); break;
+        case 12: launch(k_grid_pl<1, 2>); break;
+        case 14: launch(k_grid_pl<1, 4>); break;
+        case 21: launch(k_grid_pl<2, 1>); break;
+        case 22: launch(k_grid_pl<2, 2>); break;
+        case 24: launch(k_grid_pl<2, 4>); break;
+        case 41: launch(k_grid_pl<4, 1>); break;
+        case 42: launch(k_grid_pl<4, 2>); break;
+        default: launch(k_grid_pl<4, 4>); break;
+      }
+      YG_CUDA_TRY(cudaGetLastError());
+    }
+  } else {
   if (ev0) cudaEventRecord(ev0, st);
   for (int pol0 = 0; pol0 < v.npol; pol0 += npa) {
     g.pol0 = pol0;
@@ -2049,6 +2355,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     }
     if (e == cudaErrorInvalidConfiguration) return YG_ERR_UNSUPPORTED;
     if (e != cudaSuccess) return YG_ERR_CUDA;
+  }
   }
   if (ev1) cudaEventRecord(ev1, st);
   HaloArgs h;

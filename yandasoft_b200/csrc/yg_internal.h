@@ -110,7 +110,7 @@ struct BinArgs {
   int ntx, nty;            // tiles per axis
   int mbits;               // bits of the within-tile Morton code
   int wy;                  // row modulus of the residues in the records (0: the padded CF width)
-  int pos_major;           // also build the position-major records (rec_pos)
+  int pos_major;           // also build second-order records (rec_pos): 1 position-major, 2 plane-major
   unsigned long long invalid_key;  // one past the largest valid key
   CFView cf;
 };
@@ -140,6 +140,8 @@ struct Plan {
   DevBuf rec_pos;               // the same records ordered by tile, then position in the tile, then CF
   DevBuf pos_key2, pos_val2;    // sort buffers of rec_pos (released after the build)
   bool pos_ready = false;       // rec_pos is built
+  int pos_mode = 0;             // its order: 1 position then CF index; 2 CF plane, position, offset
+  int os2 = 1;                  // oversampling offsets per CF plane
   DevBuf ext;                   // continuous learned CF: per sorted sample (ru, rv, w, 0)
   bool ext_ready = false;
   int mbits = 0, ncf = 0;       // sort-key layout
