@@ -829,7 +829,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
 // moves it to another cell of its residue class (GridKernel::grid's sums,
 // GridKernel.cc:57-97, in another order).
 // ---------------------------------------------------------------------------
-template <int NPOL, int SL>
+template <int NPOL, int SL, int NG>
 __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nthr = blockDim.x - 32;
@@ -958,17 +958,22 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
       s_abort = 1;
     }
   } else {
-    // ---- tap warps: thread t owns x residue t mod 16 and the y residues
-    // t / 16 + RY q, q < SL (RY = ceil(Wy / SL))
+    // ---- tap warps, in NG groups of nthr / NG threads, group g accumulating
+    // the polarisations g NPOL / NG ..: thread t of a group owns x residue
+    // t mod 16 and the y residues t / 16 + RY q, q < SL (RY = ceil(Wy / SL))
+    constexpr int NPG = NPOL / NG;
+    const int gsz = nthr / NG;
+    const int grp = threadIdx.x / gsz, tl = threadIdx.x - grp * gsz;
+    const int pofs = grp * NPG;
     const int RY = (Wy + SL - 1) / SL;
-    const int rx = threadIdx.x & 15, ry0 = threadIdx.x >> 4;
+    const int rx = tl & 15, ry0 = tl >> 4;
     int rcell[SL];
-    float2 racc[SL][NPOL];
+    float2 racc[SL][NPG];
 #pragma unroll
     for (int q = 0; q < SL; ++q) {
       rcell[q] = Pg * Pg + threadIdx.x;          // this thread's trash cell until the first sample
 #pragma unroll
-      for (int p = 0; p < NPOL; ++p) racc[q][p] = make_float2(0.f, 0.f);
+      for (int p = 0; p < NPG; ++p) racc[q][p] = make_float2(0.f, 0.f);
     }
     const bool live = ry0 < RY;
     for (int nseg = 0;; ++nseg) {
@@ -981,42 +986,47 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
       const unsigned char* sp = ring + (size_t)stage * SB;
       const int cnt = *reinterpret_cast<const volatile int*>(sp + SB - 16);
       if (cnt < 0) break;
-      const int4* recs = reinterpret_cast<const int4*>(sp);
-      const float2* vs = reinterpret_cast<const float2*>(sp + kSeg * 16);
+      // the staged records, visibilities and CF plane are never written while
+      // the tile is: restrict lets the next samples' loads pass this one's stores
+      const int4* __restrict__ recs = reinterpret_cast<const int4*>(sp);
+      const float2* __restrict__ vs = reinterpret_cast<const float2*>(sp + kSeg * 16);
+      const float2* __restrict__ pb = planebuf;
+      float2* __restrict__ acc = acc_s;
       if (live) {
+#pragma unroll 2
         for (int l = 0; l < cnt; ++l) {
           const int4 r = recs[l];
           const int jx = (rx - (r.y & 1023)) & 15;
           const int my = (r.y >> 10) & 1023;
           const bool conj = a.v.pcf && r.y < 0;
-          float2 vv[NPOL];
+          float2 vv[NPG];
 #pragma unroll
-          for (int p = 0; p < NPOL; ++p) vv[p] = vs[l * NPOL + p];
+          for (int p = 0; p < NPG; ++p) vv[p] = vs[l * NPOL + pofs + p];
 #pragma unroll
           for (int q = 0; q < SL; ++q) {
             const int ry = ry0 + RY * q;
             if (SL > 1 && ry >= Wy) continue;
             int jy = ry - my;
             jy += (jy < 0) ? Wy : 0;
-            float2 c = planebuf[r.z + jy * 16 + jx];
+            float2 c = pb[r.z + jy * 16 + jx];
             if (conj) c.y = -c.y;
             const int cell = r.x + jx + Pg * jy;
             if (cell != rcell[q]) {
-              float2 g[NPOL];
+              float2 g[NPG];
 #pragma unroll
-              for (int p = 0; p < NPOL; ++p) g[p] = acc_s[p * PG2 + rcell[q]];
+              for (int p = 0; p < NPG; ++p) g[p] = acc[(pofs + p) * PG2 + rcell[q]];
 #pragma unroll
-              for (int p = 0; p < NPOL; ++p) {
+              for (int p = 0; p < NPG; ++p) {
                 g[p].x += racc[q][p].x;
                 g[p].y += racc[q][p].y;
                 racc[q][p] = make_float2(0.f, 0.f);
               }
 #pragma unroll
-              for (int p = 0; p < NPOL; ++p) acc_s[p * PG2 + rcell[q]] = g[p];
+              for (int p = 0; p < NPG; ++p) acc[(pofs + p) * PG2 + rcell[q]] = g[p];
               rcell[q] = cell;
             }
 #pragma unroll
-            for (int p = 0; p < NPOL; ++p) {
+            for (int p = 0; p < NPG; ++p) {
               racc[q][p].x = fmaf(vv[p].x, c.x, fmaf(-vv[p].y, c.y, racc[q][p].x));
               racc[q][p].y = fmaf(vv[p].x, c.y, fmaf(vv[p].y, c.x, racc[q][p].y));
             }
@@ -1029,11 +1039,11 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
 #pragma unroll
     for (int q = 0; q < SL; ++q)
 #pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        float2 g = acc_s[p * PG2 + rcell[q]];
+      for (int p = 0; p < NPG; ++p) {
+        float2 g = acc_s[(pofs + p) * PG2 + rcell[q]];
         g.x += racc[q][p].x;
         g.y += racc[q][p].y;
-        acc_s[p * PG2 + rcell[q]] = g;
+        acc_s[(pofs + p) * PG2 + rcell[q]] = g;
       }
   }
   __syncthreads();
@@ -2284,9 +2294,11 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   if (planes) {
     // k_grid_pl: tile + one plane of every oversampling offset + the ring
     const int os2 = pl.os2;
-    // layout 1: one residue row per thread; 2 and 3: two and four rows
-    const int sl = mode == 3 ? 4 : (mode == 2 ? 2 : 1);
-    const int nthr_pl = (16 * ((pl.wy + sl - 1) / sl) + 31) / 32 * 32;
+    // layout 1: one residue row per thread; 2: the same in two groups of
+    // threads, each accumulating half the polarisations; 3: two rows per thread
+    const int sl = mode == 3 ? 2 : 1;
+    const int ng = (mode == 2 && v.npol >= 2) ? 2 : 1;
+    const int nthr_pl = ng * ((16 * ((pl.wy + sl - 1) / sl) + 31) / 32 * 32);
     const size_t plane_b = ((size_t)os2 * pl.wy * 16 * sizeof(float2) + 127) & ~(size_t)127;
     g.rec = pl.rec_pos.as<int4>();
     g.pps = os2;
@@ -2313,16 +2325,17 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
         kern<<<pl.nitems, nthr_pl + 32, smem, st>>>(g);
         YG_COUNT_LAUNCH();
       };
-      switch (npa * 10 + sl) {
-        case 11: launch(k_grid_pl<1, 1>); break;
-        case 12: launch(k_grid_pl<1, 2>); break;
-        case 14: launch(k_grid_pl<1, 4>); break;
-        case 21: launch(k_grid_pl<2, 1>); break;
-        case 22: launch(k_grid_pl<2, 2>); break;
-        case 24: launch(k_grid_pl<2, 4>); break;
-        case 41: launch(k_grid_pl<4, 1>); break;
-        case 42: launch(k_grid_pl<4, 2>); break;
-        default: launch(k_grid_pl<4, 4>); break;
+      const int ngl = npa >= 2 ? ng : 1;
+      if (ngl != ng) return YG_ERR_UNSUPPORTED;
+      switch (npa * 100 + sl * 10 + ngl) {
+        case 111: launch(k_grid_pl<1, 1, 1>); break;
+        case 121: launch(k_grid_pl<1, 2, 1>); break;
+        case 211: launch(k_grid_pl<2, 1, 1>); break;
+        case 212: launch(k_grid_pl<2, 1, 2>); break;
+        case 221: launch(k_grid_pl<2, 2, 1>); break;
+        case 411: launch(k_grid_pl<4, 1, 1>); break;
+        case 412: launch(k_grid_pl<4, 1, 2>); break;
+        default: launch(k_grid_pl<4, 2, 1>); break;
       }
       YG_CUDA_TRY(cudaGetLastError());
     }
