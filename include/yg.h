@@ -173,7 +173,8 @@ int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
  * 32 as well orders each tile's samples by position before CF for gridding
  * (plans made afterwards keep both orders) and reads the taps through L2;
  * adding 64 orders them by CF plane, then position, then oversampling offset
- * and stages each plane's offsets in shared memory once (16-wide CFs). */
+ * and stages each plane's offsets in shared memory once (16-wide CFs), and
+ * 128 with it keeps that kernel's tile in global memory (two CTAs per SM). */
 int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */

@@ -413,12 +413,14 @@ def test_preconditioner_function_gridder(ygmod, oracle_mod, kind, npol):
         gd.degrid(Accessor(ds.uvw, ds.freq, np.zeros_like(ds.vis)))
 
 
-@pytest.mark.parametrize("variant,pcf", [(65, False), (65, True), (66, False), (67, True), (49, False), (17, False)])
+@pytest.mark.parametrize("variant,pcf", [(65, False), (65, True), (66, False), (67, True), (193, False), (194, True), (49, False), (17, False)])
 def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
     """The k_grid variants the autotuner may pick, each against the oracle on
     flagged, weighted, phase-rotated data with 4 polarisations: 65 (records in
     plane-major order, each CF plane's oversampling offsets staged in shared
-    memory, register accumulation; 7-wide CFs in 16-wide rows), 49
+    memory, register accumulation; 7-wide CFs in 16-wide rows), 66 and 67
+    (two polarisation groups, two rows per thread), 193 and 194 (the same
+    with the tile in global memory, reductions at each flush), 49
     (position-major records, taps through L2) and 17 (register accumulation
     over the CF-major records).  Grids 1e-5, sums of weights exact; the
     preconditioner's conjugate half through the plane-major kernel."""

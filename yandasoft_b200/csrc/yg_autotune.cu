@@ -76,7 +76,7 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   // (register accumulation over the CF-major records, 16, and position-major
   // records with taps through L2, 32, measured slower on the benchmark
   // workloads: not tried)
-  const std::vector<int> variants = {1, 65, 66, 67, 2};
+  const std::vector<int> variants = {1, 65, 193, 66, 194, 2};
   const int save_tile = tile_override_, save_vmax = vmax_, save_mode = grid_mode_;
   Chunk scratch_chunk = dc;
   DevBuf model;

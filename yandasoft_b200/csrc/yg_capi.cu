@@ -357,9 +357,10 @@ int yg_set_tile(yg_gridder* g, int32_t tile) {
 
 int yg_set_grid_variant(yg_gridder* g, int32_t variant) {
   return guarded([&] {
-    if (variant < 0 || (variant & ~112) > 3)
+    if (variant < 0 || (variant & ~240) > 3)
       throw yg::YgError{YG_ERR_ARG, "variant must be 0 to 3, plus 16 (register accumulation), 32 "
-                                    "(position-major records) or 64 (plane-major records, staged CF planes)"};
+                                    "(position-major records) or 64 (plane-major records, staged CF planes; "
+                                    "plus 128: their tile in global memory)"};
     G(g).set_grid_mode(variant);
   });
 }

@@ -829,15 +829,19 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
 // moves it to another cell of its residue class (GridKernel::grid's sums,
 // GridKernel.cc:57-97, in another order).
 // ---------------------------------------------------------------------------
-template <int NPOL, int SL, int NG>
+template <int NPOL, int SL, int NG, bool GT>
 __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nthr = blockDim.x - 32;
   const int ncw = nthr / 32;
   const int Pg = a.Pg, Wy = a.Wy, os2 = a.pps;       // pps carries os^2 in this kernel
   const int PG2 = Pg * Pg + nthr;
-  float2* acc_s = reinterpret_cast<float2*>(smem_raw);
-  size_t off = ((size_t)NPOL * PG2 * sizeof(float2) + 127) & ~(size_t)127;
+  // GT: the padded tile lives in this item's scratch slot in global memory
+  // (L2), written only by the rare flushes, as reductions; shared memory then
+  // holds the plane buffer and the ring only (two CTAs per SM)
+  float2* acc_s = GT ? a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * PG2
+                     : reinterpret_cast<float2*>(smem_raw);
+  size_t off = GT ? 0 : ((size_t)NPOL * PG2 * sizeof(float2) + 127) & ~(size_t)127;
   float2* planebuf = reinterpret_cast<float2*>(smem_raw + off);
   const int prow = Wy * 16;                           // float2 per oversampling offset
   off += ((size_t)os2 * prow * sizeof(float2) + 127) & ~(size_t)127;
@@ -1012,17 +1016,28 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
             if (conj) c.y = -c.y;
             const int cell = r.x + jx + Pg * jy;
             if (cell != rcell[q]) {
-              float2 g[NPG];
+              if (GT) {
+                // the thread owns the cell: its reductions land in program order
 #pragma unroll
-              for (int p = 0; p < NPG; ++p) g[p] = acc[(pofs + p) * PG2 + rcell[q]];
+                for (int p = 0; p < NPG; ++p) {
+                  float2* gp = acc + (pofs + p) * PG2 + rcell[q];
+                  atomicAdd(&gp->x, racc[q][p].x);
+                  atomicAdd(&gp->y, racc[q][p].y);
+                  racc[q][p] = make_float2(0.f, 0.f);
+                }
+              } else {
+                float2 g[NPG];
 #pragma unroll
-              for (int p = 0; p < NPG; ++p) {
-                g[p].x += racc[q][p].x;
-                g[p].y += racc[q][p].y;
-                racc[q][p] = make_float2(0.f, 0.f);
+                for (int p = 0; p < NPG; ++p) g[p] = acc[(pofs + p) * PG2 + rcell[q]];
+#pragma unroll
+                for (int p = 0; p < NPG; ++p) {
+                  g[p].x += racc[q][p].x;
+                  g[p].y += racc[q][p].y;
+                  racc[q][p] = make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int p = 0; p < NPG; ++p) acc[(pofs + p) * PG2 + rcell[q]] = g[p];
               }
-#pragma unroll
-              for (int p = 0; p < NPG; ++p) acc[(pofs + p) * PG2 + rcell[q]] = g[p];
               rcell[q] = cell;
             }
 #pragma unroll
@@ -1040,10 +1055,16 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     for (int q = 0; q < SL; ++q)
 #pragma unroll
       for (int p = 0; p < NPG; ++p) {
-        float2 g = acc_s[(pofs + p) * PG2 + rcell[q]];
-        g.x += racc[q][p].x;
-        g.y += racc[q][p].y;
-        acc_s[(pofs + p) * PG2 + rcell[q]] = g;
+        float2* gp = acc_s + (pofs + p) * PG2 + rcell[q];
+        if (GT) {
+          atomicAdd(&gp->x, racc[q][p].x);
+          atomicAdd(&gp->y, racc[q][p].y);
+        } else {
+          float2 g = *gp;
+          g.x += racc[q][p].x;
+          g.y += racc[q][p].y;
+          *gp = g;
+        }
       }
   }
   __syncthreads();
@@ -1051,6 +1072,7 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     if (warp == ncw && lane == 0) seg_drain(nfill, NST, full);
     return;
   }
+  if (GT) return;   // the tile is already in the scratch slot
   const int P = a.P, P2 = P * P;
   float2* out = a.scratch + ((size_t)blockIdx.x * a.npol_total + a.pol0) * P2;
   for (int i = threadIdx.x; i < NPOL * P2; i += blockDim.x) {
@@ -1201,6 +1223,8 @@ struct HaloArgs {
   int tile, ntx, nty;
   long long ntiles;
   int smax, P;
+  long long slot_pol;        // scratch elements per polarisation of an item (P^2, or the padded tile)
+  int row;                   // scratch row stride (P, or the padded tile's Pg)
 };
 
 __global__ void k_halo_sum(HaloArgs a) {
@@ -1245,7 +1269,7 @@ __global__ void k_halo_sum(HaloArgs a) {
         if (m == 0) continue;
         const int b = a.item_base[nt];
         for (int j = 0; j < m; ++j) {
-          const float2 v = a.scratch[((size_t)(b + j) * a.npol + p) * P2 + px + (size_t)a.P * py];
+          const float2 v = a.scratch[((size_t)(b + j) * a.npol + p) * a.slot_pol + px + (size_t)a.row * py];
           sum.x += v.x;
           sum.y += v.y;
           hit = true;
@@ -2194,7 +2218,14 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
                       pl.wy > 0 && pl.wy <= 16 && !cf.varsup && v.npol <= 4;
   const bool pos = !planes && (mode & 32) != 0 && pl.pos_ready && pl.pos_mode == 1 && !learned && v.npol <= 4;
   const bool racc = (mode & 16) != 0 || pos;
+  // mode 128 (with 64): the plane-major kernel's tile in the item's scratch slot
+  const bool gtile = planes && (mode & 128) != 0;
   mode &= 15;
+  // plane-major kernel layout: 1 one residue row per thread; 2 the same in two
+  // groups of threads, each accumulating half the polarisations; 3 two rows per thread
+  const int pl_sl = mode == 3 ? 2 : 1;
+  const int pl_ng = (mode == 2 && v.npol >= 2) ? 2 : 1;
+  const int gtile_nthr = planes ? pl_ng * ((16 * ((pl.wy + pl_sl - 1) / pl_sl) + 31) / 32 * 32) : 0;
   if (learned && v.pcf) return YG_ERR_UNSUPPORTED;
   if (pl.nitems == 0) return YG_OK;
   if (!cf.pad || cf.wpad <= 0) return YG_ERR_STATE;
@@ -2207,7 +2238,8 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     shape = GridShape{(16 * pl.wy + 31) / 32 * 32, 1, 16};
   }
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
-  const size_t per_item = (size_t)v.npol * P * P * sizeof(float2);
+  const size_t per_item = gtile ? (size_t)v.npol * ((size_t)Pg * Pg + gtile_nthr) * sizeof(float2)
+                                : (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
   YG_CUDA_TRY(svis.ensure((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
   if (v.npol > 4) return YG_ERR_UNSUPPORTED;
@@ -2294,11 +2326,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   if (planes) {
     // k_grid_pl: tile + one plane of every oversampling offset + the ring
     const int os2 = pl.os2;
-    // layout 1: one residue row per thread; 2: the same in two groups of
-    // threads, each accumulating half the polarisations; 3: two rows per thread
-    const int sl = mode == 3 ? 2 : 1;
-    const int ng = (mode == 2 && v.npol >= 2) ? 2 : 1;
-    const int nthr_pl = ng * ((16 * ((pl.wy + sl - 1) / sl) + 31) / 32 * 32);
+    const int sl = pl_sl, ng = pl_ng, nthr_pl = gtile_nthr;
     const size_t plane_b = ((size_t)os2 * pl.wy * 16 * sizeof(float2) + 127) & ~(size_t)127;
     g.rec = pl.rec_pos.as<int4>();
     g.pps = os2;
@@ -2306,11 +2334,14 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
     npa = 0;
     for (int c : {4, 2, 1}) {
       if (c > v.npol || v.npol % c) continue;
-      const size_t tile_b = ((size_t)c * ((size_t)Pg * Pg + nthr_pl) * sizeof(float2) + 127) & ~(size_t)127;
+      const size_t tile_b =
+          gtile ? 0 : ((size_t)c * ((size_t)Pg * Pg + nthr_pl) * sizeof(float2) + 127) & ~(size_t)127;
       const size_t stage = (size_t)seg_stage_bytes(0, c) + 16;
-      if (tile_b + plane_b + 2 * stage <= 227 * 1024) {
+      // two CTAs per SM where the tile is in global memory and the plane fits twice
+      const size_t budget = (gtile && plane_b + 2 * stage + 256 <= 113 * 1024) ? 113 * 1024 - 256 : 227 * 1024;
+      if (tile_b + plane_b + 2 * stage <= budget) {
         npa = c;
-        g.nstages = (int)std::min<size_t>(8, (227 * 1024 - tile_b - plane_b) / stage);
+        g.nstages = (int)std::min<size_t>(8, (budget - tile_b - plane_b) / stage);
         g.stage_bytes = seg_stage_bytes(0, c);
         smem = tile_b + plane_b + (size_t)g.nstages * stage;
         break;
@@ -2327,15 +2358,21 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
       };
       const int ngl = npa >= 2 ? ng : 1;
       if (ngl != ng) return YG_ERR_UNSUPPORTED;
-      switch (npa * 100 + sl * 10 + ngl) {
-        case 111: launch(k_grid_pl<1, 1, 1>); break;
-        case 121: launch(k_grid_pl<1, 2, 1>); break;
-        case 211: launch(k_grid_pl<2, 1, 1>); break;
-        case 212: launch(k_grid_pl<2, 1, 2>); break;
-        case 221: launch(k_grid_pl<2, 2, 1>); break;
-        case 411: launch(k_grid_pl<4, 1, 1>); break;
-        case 412: launch(k_grid_pl<4, 1, 2>); break;
-        default: launch(k_grid_pl<4, 2, 1>); break;
+      switch (npa * 100 + sl * 10 + ngl + (gtile ? 1000 : 0)) {
+        case 111: launch(k_grid_pl<1, 1, 1, false>); break;
+        case 121: launch(k_grid_pl<1, 2, 1, false>); break;
+        case 211: launch(k_grid_pl<2, 1, 1, false>); break;
+        case 212: launch(k_grid_pl<2, 1, 2, false>); break;
+        case 221: launch(k_grid_pl<2, 2, 1, false>); break;
+        case 411: launch(k_grid_pl<4, 1, 1, false>); break;
+        case 412: launch(k_grid_pl<4, 1, 2, false>); break;
+        case 421: launch(k_grid_pl<4, 2, 1, false>); break;
+        case 1111: launch(k_grid_pl<1, 1, 1, true>); break;
+        case 1211: launch(k_grid_pl<2, 1, 1, true>); break;
+        case 1212: launch(k_grid_pl<2, 1, 2, true>); break;
+        case 1411: launch(k_grid_pl<4, 1, 1, true>); break;
+        case 1412: launch(k_grid_pl<4, 1, 2, true>); break;
+        default: return YG_ERR_UNSUPPORTED;
       }
       YG_CUDA_TRY(cudaGetLastError());
     }
@@ -2386,6 +2423,8 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   h.ntiles = (long long)pl.ntx * pl.nty;
   h.smax = pl.smax;
   h.P = P;
+  h.slot_pol = gtile ? (long long)Pg * Pg + gtile_nthr : (long long)P * P;
+  h.row = gtile ? Pg : P;
   const long long nblocks = pl.ntiles_total;
   if (nblocks > 0x7fffffffll) return YG_ERR_UNSUPPORTED;
   k_halo_sum<<<(unsigned)nblocks, 256, 0, st>>>(h);
