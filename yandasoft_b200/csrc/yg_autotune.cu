@@ -71,12 +71,14 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   std::vector<int> vmaxes = {def_vmax};
   for (int v : {def_vmax / 4, def_vmax * 4})
     if (v >= 128 && v <= (1 << 20)) vmaxes.push_back(v);
-  // thread layouts: the default; the plane-major records with staged CF
-  // planes and one, two or four residue rows per thread; half the threads
-  // (register accumulation over the CF-major records, 16, and position-major
-  // records with taps through L2, 32, measured slower on the benchmark
-  // workloads: not tried)
-  const std::vector<int> variants = {1, 65, 193, 66, 194, 2};
+  // thread layouts: the default; for 16-wide CFs the plane-major records with
+  // staged CF planes (tile in global memory, 193, or in shared memory, 65;
+  // two polarisation groups, 194), half the threads, tap sums in registers
+  // over the CF-major records (17); for wider CFs the default, 17 and half
+  // the threads.  Position-major records with taps through L2 (32) measured
+  // slower on the benchmark workloads and are not tried.
+  const std::vector<int> variants =
+      wpad == 16 ? std::vector<int>{1, 193, 65, 194, 2, 17} : std::vector<int>{1, 17, 2};
   const int save_tile = tile_override_, save_vmax = vmax_, save_mode = grid_mode_;
   Chunk scratch_chunk = dc;
   DevBuf model;
@@ -131,11 +133,13 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
   // first the tile with the default layout and work-item size (the default
   // itself first), then the other layouts at the best tile, then the
   // work-item size around the best of those
-  for (int t : tiles)
-    if (trials < max_trials) trial(t, def_vmax, variants[0]);
-  const int lead_tile = rep.best.tile;
-  for (size_t k = 1; k < variants.size(); ++k)
-    if (trials < max_trials && lead_tile > 0) trial(lead_tile, def_vmax, variants[k]);
+  // the layouts at the default tile (the default first), then the other tiles
+  // with the best layout, then the work-item size around the best of those
+  for (int v : variants)
+    if (trials < max_trials) trial(tiles[0], def_vmax, v);
+  const int lead_variant = rep.best.variant;
+  for (size_t k = 1; k < tiles.size(); ++k)
+    if (trials < max_trials) trial(tiles[k], def_vmax, lead_variant);
   const TuneChoice lead = rep.best;
   for (int vm : vmaxes)
     if (vm != def_vmax && trials < max_trials && lead.tile > 0) trial(lead.tile, vm, lead.variant);

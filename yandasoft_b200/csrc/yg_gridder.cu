@@ -397,7 +397,7 @@ std::unique_ptr<Gridder> Gridder::clone() const {
 }
 
 Gridder::~Gridder() {
-  for (cudaStream_t* cs : {&copy_stream_, &down_stream_}) {
+  for (cudaStream_t* cs : {&copy_stream_, &down_stream_, &bin_stream_}) {
     if (*cs) {
       cudaStreamSynchronize(*cs);
       cudaStreamDestroy(*cs);
@@ -408,6 +408,9 @@ Gridder::~Gridder() {
   for (auto& e : piece_down_)
     if (e) cudaEventDestroy(e);
   if (piece_done_) cudaEventDestroy(piece_done_);
+  for (auto& e : piece_pass_)
+    if (e) cudaEventDestroy(e);
+  if (piece_binned_) cudaEventDestroy(piece_binned_);
   if (stream_) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
@@ -425,11 +428,12 @@ __global__ void k_error_out(const DevError* __restrict__ d, DevError* h) {
   h->where = d->where;
 }
 
-void Gridder::check_error() {
+void Gridder::check_error(cudaStream_t st) {
+  if (!st) st = stream_;
   cuda_check(err_h_.ensure(sizeof(DevError)), "alloc error mirror");
-  k_error_out<<<1, 1, 0, stream_>>>(err_.as<DevError>(), err_h_.as<DevError>());
+  k_error_out<<<1, 1, 0, st>>>(err_.as<DevError>(), err_h_.as<DevError>());
   cuda_check(cudaGetLastError(), "error readback");
-  cuda_check(cudaStreamSynchronize(stream_), "kernel execution");
+  cuda_check(cudaStreamSynchronize(st), "kernel execution");
   DevError h{};
   h.code = err_h_.as<volatile DevError>()->code;
   h.where = err_h_.as<volatile DevError>()->where;
@@ -845,7 +849,8 @@ std::vector<uint8_t> Gridder::psf_rows(const Chunk& c) {
   return ok;
 }
 
-void Gridder::bin(const Chunk& dc, Plan& pl) {
+void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st) {
+  if (!st) st = stream_;
   throw_if(dc.npol != npol_, YG_ERR_UNSUPPORTED,
            "visibility and image polarisation frames must match (no polarisation conversion)");
   const std::vector<double> freqs = host_freqs(dc);
@@ -856,12 +861,12 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
   }
   const std::vector<int> cmap = chan_map(freqs.data(), dc.nchan);
   cuda_check(pl.chanmap.ensure(std::max(1, dc.nchan) * sizeof(int)), "alloc");
-  cuda_check(cudaMemcpyAsync(pl.chanmap.p, cmap.data(), dc.nchan * sizeof(int), cudaMemcpyHostToDevice, stream_), "up");
+  cuda_check(cudaMemcpyAsync(pl.chanmap.p, cmap.data(), dc.nchan * sizeof(int), cudaMemcpyHostToDevice, st), "up");
   std::vector<uint8_t> rows = psf_rows(dc);
   const uint8_t* row_ok = nullptr;
   if (!rows.empty()) {
     cuda_check(rowok_d_.ensure(rows.size()), "alloc");
-    cuda_check(cudaMemcpyAsync(rowok_d_.p, rows.data(), rows.size(), cudaMemcpyHostToDevice, stream_), "up");
+    cuda_check(cudaMemcpyAsync(rowok_d_.p, rows.data(), rows.size(), cudaMemcpyHostToDevice, st), "up");
     row_ok = rowok_d_.as<uint8_t>();
   }
   BinArgs a;
@@ -876,8 +881,8 @@ void Gridder::bin(const Chunk& dc, Plan& pl) {
     const long long n = dc.nrow * (long long)dc.nchan;
     vmax = (int)std::min<long long>(1 << 20, std::max<long long>(512, n / (148 * 8)));
   }
-  rc_check(plan_build(pl, a, vmax, err_.as<DevError>(), stream_), "binning");
-  check_error();
+  rc_check(plan_build(pl, a, vmax, err_.as<DevError>(), st), "binning");
+  check_error(st);
 }
 
 static VisArgs vis_args(const Chunk& dc, const float* mfs, bool psf, bool pcf = false) {
@@ -949,48 +954,74 @@ Chunk Gridder::stage_rows(const Chunk& c, long long r0, long long nr, int b, boo
 }
 
 void Gridder::run_pieces(Chunk& c, bool degridding) {
-  if (!copy_stream_) cuda_check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "stream");
-  if (degridding && !down_stream_) {
-    cuda_check(cudaStreamCreateWithFlags(&down_stream_, cudaStreamNonBlocking), "stream");
-    cuda_check(cudaEventCreateWithFlags(&piece_done_, cudaEventDisableTiming), "event");
-    for (auto& e : piece_down_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-  }
+  auto stream = [&](cudaStream_t& cs) {
+    if (!cs) cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+  };
+  auto event = [&](cudaEvent_t& e) {
+    if (!e) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  };
+  stream(copy_stream_);
+  stream(bin_stream_);
+  if (degridding) stream(down_stream_);
+  for (auto& e : piece_down_) event(e);
+  for (auto& e : piece_pass_) event(e);
+  event(piece_binned_);
   const double bytes = (double)c.nrow * c.nchan * c.npol * sizeof(float2);
   const int K = (int)std::max(2.0, std::min(16.0, std::ceil(bytes / kPipePieceBytes)));
   const long long rows = (c.nrow + K - 1) / K;
   const int npieces = (int)((c.nrow + rows - 1) / rows);
+  // Each piece: upload (copy stream) -> binning (bin stream; the host waits
+  // for its item count) -> pass (the gridder's stream) -> download (degrid,
+  // its own stream).  Piece k + 1 is uploaded and binned while the pass over
+  // piece k runs; a staging buffer and its plan are reused once the pass two
+  // pieces back (and its download) is done.  Passes stay in row order on one
+  // stream, so sums of weights and the carried value of off-grid samples are
+  // those of one call; device errors are read once at the end.
   std::vector<Chunk> staged(2);
-  staged[0] = stage_rows(c, 0, std::min(rows, c.nrow), 0, true);
+  auto stage_and_bin = [&](int k) {
+    const int b = k & 1;
+    const long long r0 = k * rows;
+    cuda_check(cudaStreamWaitEvent(copy_stream_, piece_pass_[b], 0), "wait pass");
+    staged[b] = stage_rows(c, r0, std::min(rows, c.nrow - r0), b, true);
+    cuda_check(cudaStreamWaitEvent(bin_stream_, piece_up_[b], 0), "wait upload");
+    cuda_check(cudaStreamWaitEvent(bin_stream_, piece_pass_[b], 0), "wait pass");
+    init_cf(staged[b]);
+    bin(staged[b], piece_plan_[b], bin_stream_);
+    cuda_check(cudaEventRecord(piece_binned_, bin_stream_), "event");
+  };
+  // no pass has used the buffers yet: their pass events complete at once
+  for (auto& e : piece_pass_) cuda_check(cudaEventRecord(e, stream_), "event");
+  stage_and_bin(0);
   for (int k = 0; k < npieces; ++k) {
     const int b = k & 1;
     const long long r0 = k * rows, nr = std::min(rows, c.nrow - r0);
-    if (k + 1 < npieces) {
-      // buffer b ^ 1 was last used by piece k - 1, which has finished (the
-      // passes below end on a host synchronisation); the upload waits for
-      // that piece's download (stage_rows)
-      const long long r1 = (k + 1) * rows;
-      staged[b ^ 1] = stage_rows(c, r1, std::min(rows, c.nrow - r1), b ^ 1, true);
-    }
-    // the gridder's stream waits for this piece's upload; the next piece's
-    // upload runs on (binning takes the frequencies from the caller's host array)
-    cuda_check(cudaStreamWaitEvent(stream_, piece_up_[b], 0), "wait upload");
     Chunk& dc = staged[b];
-    init_cf(dc);
-    bin(dc, piece_plan_[b]);
+    Plan& pl = piece_plan_[b];
+    cuda_check(cudaStreamWaitEvent(stream_, piece_binned_, 0), "wait binning");
+    const float* mfs = mfs_weights(dc);
+    const double w = 2.0 * cf_.support + 1.0;
     if (degridding) {
-      degrid_plan(dc, piece_plan_[b]);
+      degrid_enqueue(dc, pl, mfs, stream_);
+      stats_.samples_degridded += (double)pl.nvalid * dc.npol;
+      stats_.taps_degridded += (double)pl.nvalid * dc.npol * w * w;
+    } else {
+      grid_enqueue(dc, pl, mfs, stream_);
+      stats_.samples_gridded += (double)pl.nvalid * dc.npol;
+      stats_.taps_gridded += (double)pl.nvalid * dc.npol * w * w;
+    }
+    cuda_check(cudaEventRecord(piece_pass_[b], stream_), "event");
+    if (degridding) {
       // the download runs on a stream of its own, beside the next upload
-      cuda_check(cudaEventRecord(piece_done_, stream_), "event");
-      cuda_check(cudaStreamWaitEvent(down_stream_, piece_done_, 0), "wait degrid");
+      cuda_check(cudaStreamWaitEvent(down_stream_, piece_pass_[b], 0), "wait degrid");
       cuda_check(cudaMemcpy2DAsync((char*)c.vis + r0 * sizeof(float2), (size_t)c.nrow * sizeof(float2), dc.vis,
                                    (size_t)nr * sizeof(float2), (size_t)nr * sizeof(float2),
                                    (size_t)c.nchan * c.npol, cudaMemcpyDeviceToHost, down_stream_),
                  "download rows");
       cuda_check(cudaEventRecord(piece_down_[b], down_stream_), "event");
-    } else {
-      grid_plan(dc, piece_plan_[b]);
     }
+    if (k + 1 < npieces) stage_and_bin(k + 1);
   }
+  check_error();
   cuda_check(cudaStreamSynchronize(copy_stream_), "pieces");
   if (degridding) cuda_check(cudaStreamSynchronize(down_stream_), "pieces");
 }

@@ -129,7 +129,7 @@ class Gridder {
   float2* device_grid() { return grids_.as<float2>(); }
   cudaStream_t stream() const { return stream_; }
   // plan-level API for repeated passes over the same data
-  void bin(const Chunk& c, Plan& pl);
+  void bin(const Chunk& c, Plan& pl, cudaStream_t st = nullptr);
   void grid_plan(const Chunk& c, const Plan& pl);
   void degrid_plan(Chunk& c, Plan& pl);
   // launch-only cores of grid_plan / degrid_plan: no host synchronisation,
@@ -180,7 +180,7 @@ class Gridder {
   void init_axes(const Axes& axes, int nx, int ny, int npol, int nchan);
   void init_sumw();
   void init_cf(const Chunk& dc);
-  void check_error();
+  void check_error(cudaStream_t st = nullptr);
   void upload_chunk(const Chunk& c, Chunk& dc, bool need_vis, bool vis_writable);
   std::vector<int> chan_map(const double* freq_host, int nchan) const;
   void fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, const uint8_t* row_ok) const;
@@ -275,6 +275,9 @@ class Gridder {
   cudaEvent_t piece_up_[2] = {nullptr, nullptr};
   cudaEvent_t piece_down_[2] = {nullptr, nullptr};
   cudaEvent_t piece_done_ = nullptr;
+  cudaStream_t bin_stream_ = nullptr;    // binning of the next host piece, beside the current pass
+  cudaEvent_t piece_pass_[2] = {nullptr, nullptr};   // pass over a staging buffer done
+  cudaEvent_t piece_binned_ = nullptr;
   bool pipelined(const Chunk& c) const;
   Chunk stage_rows(const Chunk& c, long long r0, long long nr, int b, bool need_vis);
   void run_pieces(Chunk& c, bool degridding);
