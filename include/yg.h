@@ -174,7 +174,10 @@ int yg_set_item_size(yg_gridder* g, int32_t vmax); /* samples per work item */
  * (plans made afterwards keep both orders) and reads the taps through L2;
  * adding 64 orders them by CF plane, then position, then oversampling offset
  * and stages each plane's offsets in shared memory once (16-wide CFs), and
- * 128 with it keeps that kernel's tile in global memory (two CTAs per SM). */
+ * 128 with it keeps that kernel's tile in global memory (two CTAs per SM).
+ * Adding 256 degrids 16-wide CFs with the CF read per tap from the segment
+ * ring (k_degrid_t) instead of the default register-held CF column; adding
+ * 512 has the default degrid one sample per half-warp pass instead of two. */
 int yg_set_grid_variant(yg_gridder* g, int32_t variant);
 int yg_synchronize(yg_gridder* g);
 /* the cudaStream_t every kernel of this handle is launched on */
@@ -250,6 +253,15 @@ int yg_mlp_loss_grad(const float* params, const float* x, const float* t, int64_
                      double* loss);
 /* y (n x 2) of the network with params rounded to FP16, host arrays */
 int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y);
+
+/* The plan builder's device primitives on host arrays (no reference
+ * counterpart: the reference grids samples in accessor order and sorts
+ * nothing).  yg_sort_pairs sorts (keys[i], vals[i]) in place by bits
+ * [0, end_bit) of the key, stably; yg_scan_i32 writes the inclusive (or, with
+ * exclusive != 0, exclusive) scan of in under op 0 = sum, 1 = min, 2 = max;
+ * in == out is allowed.  n < 2^31. */
+int yg_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, int32_t end_bit);
+int yg_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t op, int32_t exclusive);
 
 /* ---- major cycle as a CUDA graph ----
  * The caller's major-cycle sequence of ImageFFTEquation::calcImagingEquations

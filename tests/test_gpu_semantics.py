@@ -446,3 +446,43 @@ def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
     err = rel_l2(gpu, ref)
     assert err < TOL, err
     assert np.array_equal(gg.sum_weights(), og.sumw)
+
+
+@pytest.mark.parametrize("variant,npol", [(0, 4), (256, 4), (0, 2), (0, 1), (256, 1)])
+def test_degrid_kernels_against_oracle(ygmod, oracle_mod, variant, npol):
+    """Both degrid kernels of 16-wide CFs against the oracle on flagged,
+    phase-rotated data: the default (each lane keeps its column of the
+    segment's CF plane in registers, two samples per warp pass, one per
+    half-warp) and variant 256 (the CF read from the segment ring per tap).
+    Segments of odd length leave one half-warp idle on their last pass; the
+    run lengths here are mostly short and odd.  Visibilities 1e-5, added
+    into a non-zero starting cube as the reference adds them."""
+    from yandasoft_b200.gridder import Accessor, Axes
+    import oracle
+    ds = _data(npol=npol, nchan=4, seed=71, duration=240.0)
+    flag, noise, delay = _flags_noise_delay(ds, seed=17)
+    wmax = _wmax(ds.uvw, ds.freq)
+    nx, cell = 1024, 6.0 * ARCSEC
+    params = {"wmax": wmax, "nwstacks": 5, "nwplanes": 9, "oversample": 8, "maxsupport": 512}
+    og, gg = make_pair("WStackWProject", params, oracle_kw={"nwstacks": 5})
+    gg.initialiseGrid(Axes(cell, cell), (nx, nx, npol, 1))
+    og.initialise_grid(nx, nx, npol, 1, cell, cell)
+    model = _point_model(nx, npol, 1, seed=3, n=40)
+    gd = gg.clone()
+    gd.set_grid_variant(variant)
+    gd.initialiseDegrid(Axes(cell, cell), model)
+    assert gd.support()[0] <= 7
+    rng = np.random.default_rng(2)
+    start = np.asfortranarray((rng.standard_normal(ds.vis.shape) + 1j * rng.standard_normal(ds.vis.shape))
+                              .astype(np.complex64))
+    vg = np.asfortranarray(start.copy())
+    gd.degrid(Accessor(ds.uvw, ds.freq, vg, noise=noise, flag=flag, delay=delay))
+    og.grids = [np.asfortranarray(g) for g in gd.grids()]
+    og.model_empty = False
+    og.carry = None
+    vc = np.asfortranarray(start.copy())
+    og.degrid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=vc, noise=noise, flag=flag, delay=delay))
+    assert rel_l2(vc, start) > 1e-3
+    err = rel_l2(vg - start, vc - start)
+    assert err < TOL, err
+    assert rel_l2(vg, vc) < TOL

@@ -20,7 +20,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["yg_gridding.cu", "yg_cf.cu", "yg_image.cu", "yg_gridder.cu", "yg_capi.cu", "yg_spheroidal.cpp",
            "yg_noalloc.cu", "yg_learned.cu", "yg_cycle.cu",
-           "yg_autotune.cu"]
+           "yg_autotune.cu", "yg_sort.cu"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(HERE, "..", "include")]
 

@@ -130,9 +130,6 @@ TuneReport Gridder::autotune(const Chunk& dc, int max_trials) {
     }
     if (t == def_tile && vm == def_vmax && v == 1) rep.default_ms = ms;
   };
-  // first the tile with the default layout and work-item size (the default
-  // itself first), then the other layouts at the best tile, then the
-  // work-item size around the best of those
   // the layouts at the default tile (the default first), then the other tiles
   // with the best layout, then the work-item size around the best of those
   for (int v : variants)

@@ -12,6 +12,7 @@
 #include "../../include/yg.h"
 #include "yg_cycle.h"
 #include "yg_gridder.h"
+#include "yg_sort.h"
 
 struct yg_gridder {
   std::unique_ptr<yg::Gridder> g;
@@ -357,10 +358,11 @@ int yg_set_tile(yg_gridder* g, int32_t tile) {
 
 int yg_set_grid_variant(yg_gridder* g, int32_t variant) {
   return guarded([&] {
-    if (variant < 0 || (variant & ~240) > 3)
+    if (variant < 0 || (variant & ~(240 | 256 | 512)) > 3)
       throw yg::YgError{YG_ERR_ARG, "variant must be 0 to 3, plus 16 (register accumulation), 32 "
                                     "(position-major records) or 64 (plane-major records, staged CF planes; "
-                                    "plus 128: their tile in global memory)"};
+                                    "plus 128: their tile in global memory), plus 256 (degridding by "
+                                    "k_degrid_t) or 512 (one degridded sample per half-warp pass)"};
     G(g).set_grid_mode(variant);
   });
 }
@@ -484,6 +486,49 @@ int yg_mlp_eval(const float* params, const float* x, int64_t n, float* y) {
     const int rc = yg::mlp_eval_batch(net.w16.as<__half>(), X.as<float>(), n, Y.as<float>(), 0);
     if (rc) throw yg::YgError{rc, "network evaluation"};
     if (n > 0) ck(cudaMemcpy(y, Y.p, n * 2 * sizeof(float), cudaMemcpyDeviceToHost));
+  });
+}
+
+int yg_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, int32_t end_bit) {
+  return guarded([&] {
+    if (n < 0 || end_bit < 0 || end_bit > 64 || (n > 0 && (!keys || !vals)))
+      throw yg::YgError{YG_ERR_ARG, "keys and vals must be given, 0 <= end_bit <= 64"};
+    if (n >= (1ll << 31)) throw yg::YgError{YG_ERR_ARG, "n must be below 2^31"};
+    if (n == 0) return;
+    yg::DevBuf k0, k1, v0, v1, tmp;
+    auto ck = [](cudaError_t e) {
+      if (e != cudaSuccess) throw yg::YgError{YG_ERR_CUDA, cudaGetErrorString(e)};
+    };
+    ck(k0.ensure(n * 8));
+    ck(k1.ensure(n * 8));
+    ck(v0.ensure(n * 4));
+    ck(v1.ensure(n * 4));
+    ck(tmp.ensure(yg::sort_pairs_tmp_bytes(n)));
+    ck(cudaMemcpy(k0.p, keys, n * 8, cudaMemcpyHostToDevice));
+    ck(cudaMemcpy(v0.p, vals, n * 4, cudaMemcpyHostToDevice));
+    int alt = 0;
+    ck(yg::sort_pairs(k0.as<unsigned long long>(), k1.as<unsigned long long>(), v0.as<unsigned int>(),
+                      v1.as<unsigned int>(), n, end_bit, tmp.p, tmp.bytes, 0, &alt));
+    ck(cudaMemcpy(keys, alt ? k1.p : k0.p, n * 8, cudaMemcpyDeviceToHost));
+    ck(cudaMemcpy(vals, alt ? v1.p : v0.p, n * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+int yg_scan_i32(const int32_t* in, int32_t* out, int64_t n, int32_t op, int32_t exclusive) {
+  return guarded([&] {
+    if (n < 0 || op < 0 || op > 2 || (n > 0 && (!in || !out)))
+      throw yg::YgError{YG_ERR_ARG, "in and out must be given, op 0 (sum), 1 (min) or 2 (max)"};
+    if (n >= (1ll << 31)) throw yg::YgError{YG_ERR_ARG, "n must be below 2^31"};
+    if (n == 0) return;
+    yg::DevBuf a, tmp;
+    auto ck = [](cudaError_t e) {
+      if (e != cudaSuccess) throw yg::YgError{YG_ERR_CUDA, cudaGetErrorString(e)};
+    };
+    ck(a.ensure(n * 4));
+    ck(tmp.ensure(yg::scan_tmp_bytes(n)));
+    ck(cudaMemcpy(a.p, in, n * 4, cudaMemcpyHostToDevice));
+    ck(yg::scan_i32(a.as<int>(), a.as<int>(), n, op, exclusive != 0, tmp.p, tmp.bytes, 0));
+    ck(cudaMemcpy(out, a.p, n * 4, cudaMemcpyDeviceToHost));
   });
 }
 

@@ -1143,7 +1143,8 @@ void Gridder::degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t
   VisArgs v = vis_args(dc, mfs, false);
   const LearnedCF lcf = learned_view_for(dc, pl);
   rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
-                       carry_.as<float2>(), err_.as<DevError>(), st, k0, k1, cf_form_ != 0 ? &lcf : nullptr),
+                       carry_.as<float2>(), err_.as<DevError>(), st, k0, k1, cf_form_ != 0 ? &lcf : nullptr,
+                       grid_variant()),
            "degridding");
 }
 

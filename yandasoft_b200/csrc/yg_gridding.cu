@@ -6,7 +6,7 @@
 //                  (TableVisGridder.cc:604-764), and a 64-bit sort key
 //                  (grid plane, image channel, uv tile, CF index, Morton
 //                  position inside the tile).
-//   radix sort     cub::DeviceRadixSort (library call) of (key, sample id).
+//   radix sort     stable LSD radix sort of (key, sample id) (yg_sort.cu).
 //   k_tile_bounds  start/end of every tile's run in the sorted list.
 //   work items     tiles split into items of at most vmax samples.
 //   k_grid         one CTA per item: the padded tile (T + 2 Smax)^2 lives in
@@ -22,18 +22,17 @@
 //                  memory, one warp per visibility, warp-shuffle reduction.
 //   k_degrid_writeback  the reference's write-back semantics, including the
 //                  value it carries into off-grid samples.
-#include <cub/cub.cuh>
-
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
 
 #include "yg_internal.h"
 #include "yg_mlp.cuh"
+#include "yg_sort.h"
 
 namespace yg {
 
-// number of this library's own kernel launches (cub's are not counted)
+// number of this library's own kernel launches
 std::atomic<long long> g_kernel_launches{0};
 #define YG_COUNT_LAUNCH() g_kernel_launches.fetch_add(1, std::memory_order_relaxed)
 
@@ -1133,8 +1132,8 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
       const unsigned nr32 = (unsigned)v.nrow;       // plans hold fewer than 2^31 samples
       const int chan = (int)((unsigned)r.w / nr32);
       const long long row = (long long)((unsigned)r.w - (unsigned)chan * nr32);
-      float pr, pi;
-      phasor_of(v, row, chan, &pr, &pi);
+      float pr = 1.f, pi = 0.f;
+      if (out) phasor_of(v, row, chan, &pr, &pi);
       const float m = v.mfs ? v.mfs[chan] : 1.f;
       bool good = true;
 #pragma unroll
@@ -1144,6 +1143,7 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
         const float wt = noise_weight(nre);
         if (!(wt > 0.f)) good = false;
         wts[p] = wt;
+        if (!out) continue;   // checks and sums of weights only
         float2 o;
         if (v.pcf) {
           // uVis = wt: the preconditioner ignores the MFS weight
@@ -1161,7 +1161,7 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
           ri = __fmul_rn(__fmul_rn(ri, wt), m);
           o = make_float2(rr, ri);
         }
-        if (out) out[(size_t)i * v.npol + p] = o;
+        out[(size_t)i * v.npol + p] = o;
       }
       if (!good) raise_error(err, YG_ERR_WEIGHT, s);
       if (sw.sumw && good) {
@@ -1189,6 +1189,64 @@ __global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long 
         if (lane - off >= seg0) x += y;
       }
       if (tail && bin >= 0) atomicAdd(&sw.sumw[bin + (long long)sw.nrows * p], x);
+    }
+  }
+}
+
+// inv[rec[i].w] = i: the sorted index of every on-grid sample (the caller
+// sets the others to -1)
+__global__ void k_inverse(const int4* __restrict__ rec, long long nvalid, int* __restrict__ inv) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x)
+    inv[rec[i].w] = (int)i;
+}
+
+// The weighted visibilities of k_gather_vis (same arithmetic), read in the
+// cube's own order (sample s = row + nrow * chan, one thread per sample, so
+// each polarisation plane is read in coalesced runs) and written to the
+// sample's sorted slot inv[s] (its npol values are one contiguous 8 npol-byte
+// block).  The weight checks and the sums of weights stay with k_gather_vis
+// over the sorted records, where equal sum-of-weights rows come in runs.
+__global__ void k_gather_cube(VisArgs v, const int* __restrict__ inv, float2* __restrict__ out) {
+  const long long n = v.nrow * (long long)v.nchan;
+  const unsigned nr32 = (unsigned)v.nrow;       // plans hold fewer than 2^31 samples
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+    const int i = inv[s];
+    if (i < 0) continue;
+    const int chan = (int)((unsigned)s / nr32);
+    const long long row = (long long)((unsigned)s - (unsigned)chan * nr32);
+    float pr = 1.f, pi = 0.f;
+    if (!v.psf && !v.pcf) phasor_of(v, row, chan, &pr, &pi);
+    const float m = v.mfs ? v.mfs[chan] : 1.f;
+    float2 o[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      if (p >= v.npol) break;
+      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
+      const float wt = noise_weight(nre);
+      if (v.pcf) {
+        o[p] = make_float2(__fmul_rn(1.f, wt), __fmul_rn(0.f, wt));
+      } else if (v.psf) {
+        o[p] = make_float2(__fmul_rn(__fmul_rn(1.f, wt), m), __fmul_rn(__fmul_rn(0.f, wt), m));
+      } else {
+        const float2 vv = v.vis[s + n * p];
+        const float vr = vv.x, vi = -vv.y;
+        float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+        float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+        rr = __fmul_rn(__fmul_rn(rr, wt), m);
+        ri = __fmul_rn(__fmul_rn(ri, wt), m);
+        o[p] = make_float2(rr, ri);
+      }
+    }
+    float2* dst = out + (size_t)i * v.npol;
+    if (v.npol == 4) {
+      reinterpret_cast<float4*>(dst)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+      reinterpret_cast<float4*>(dst)[1] = make_float4(o[2].x, o[2].y, o[3].x, o[3].y);
+    } else if (v.npol == 2) {
+      reinterpret_cast<float4*>(dst)[0] = make_float4(o[0].x, o[0].y, o[1].x, o[1].y);
+    } else {
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        if (p < v.npol) dst[p] = o[p];
     }
   }
 }
@@ -1663,6 +1721,192 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   if (s_abort && warp == ncw && lane == 0) seg_drain(nfill, NST, full);
 }
 
+// Sum of V values per lane over the 16 lanes of each half-warp, transposed
+// as in warp_transpose_sum: value v of a half ends in its lanes with
+// (lane & 15) >> (4 - log2 V) == v.
+template <int V>
+__device__ __forceinline__ float half_transpose_sum(float (&x)[V], int lane) {
+  static_assert(V == 2 || V == 4 || V == 8 || V == 16, "2, 4, 8 or 16 values");
+  int off = 8;
+#pragma unroll
+  for (int h = V / 2; h >= 1; h /= 2) {
+    const bool up = (lane & off) != 0;
+#pragma unroll
+    for (int k = 0; k < h; ++k) {
+      const float send = up ? x[k] : x[k + h];
+      const float keep = up ? x[k + h] : x[k];
+      x[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+    off >>= 1;
+  }
+  float y = x[0];
+#pragma unroll
+  for (; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+  return y;
+}
+
+// GridKernel::degrid (GridKernel.cc:99-137) for 16-wide CF planes without the
+// learned CF: k_degrid_t's item, tile and segment ring, with the tap warps
+// working differently.  Each warp owns every ncw-th segment (one CF plane,
+// up to kSeg samples) and takes its samples two at a time, one per
+// half-warp: lane jx = lane & 15 of a half walks the rows of its sample's
+// footprint (one 16-wide grid row per half-warp load, which is one
+// shared-memory wavefront per 64-bit load), and keeps the column jx of the
+// segment's CF plane, rows 0..w-1, in registers, read once per segment rather
+// than once per sample and tap.  Rows past the CF width w are not visited.
+// SPH = 2: each half-warp takes two samples at a time (four per warp pass),
+// whose independent sums keep twice the loads in flight.
+template <int NPOL, int SPH>
+__global__ void __launch_bounds__(288) k_degrid_r(DegridTArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int Wp = 16;
+  const int Pg = a.Pg, PG2 = Pg * Pg;
+  float2* g_s = reinterpret_cast<float2*>(smem_raw);
+  unsigned char* ring = smem_raw + (size_t)NPOL * PG2 * sizeof(float2);
+  ring = reinterpret_cast<unsigned char*>((reinterpret_cast<size_t>(ring) + 127) & ~(size_t)127);
+  const int SB = a.stage_bytes, NST = a.nstages;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + (size_t)NST * SB);
+  unsigned long long* empty = full + NST;
+  __shared__ int s_abort;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int ncw = (blockDim.x >> 5) - 1;
+
+  const int4 it = a.items[blockIdx.x];
+  const long long gc = (long long)it.x / a.ntiles;
+  const long long t = (long long)it.x % a.ntiles;
+  const int tx = (int)(t % a.ntx), ty = (int)(t / a.ntx);
+  const int X0 = tx * a.tile - a.smax, Y0 = ty * a.tile - a.smax;
+  const int gind = (int)(gc / a.nchan_img), ichan = (int)(gc % a.nchan_img);
+  const long long plane_cells = (long long)a.nx * a.ny;
+  const float2* gbase = a.grid + (size_t)gind * plane_cells * NPOL * a.nchan_img + plane_cells * ((size_t)NPOL * ichan);
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], 1);
+    }
+    mbar_fence_init();
+  }
+  for (int i = threadIdx.x; i < NPOL * PG2; i += blockDim.x) {
+    const int p = i / PG2, c = i % PG2;
+    const int x = X0 + c % Pg, y = Y0 + c / Pg;
+    float2 g = make_float2(0.f, 0.f);
+    if (x >= 0 && y >= 0 && x < a.nx && y < a.ny) g = gbase[plane_cells * p + x + (size_t)a.nx * y];
+    g_s[i] = g;
+  }
+  __syncthreads();
+
+  int nfill = 0;
+  if (warp == ncw) {
+    if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp * Wp, a.cfbuf, SB, NST, ring, full, empty, nfill,
+                        true, nullptr, ncw)) {
+      if (lane == 0) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+      }
+    }
+  } else {
+    const int jx = lane & 15, half = lane >> 4;
+    constexpr int V = 2 * NPOL * SPH;
+    constexpr int sh = V == 16 ? 0 : (V == 8 ? 1 : (V == 4 ? 2 : 3));   // 4 - log2(V)
+    for (int nseg = warp;; nseg += ncw) {
+      const int stage = nseg % NST;
+      if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
+        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        s_abort = 1;
+        break;
+      }
+      const unsigned char* sp = ring + (size_t)stage * SB;
+      const volatile int* hdr = reinterpret_cast<const volatile int*>(sp + SB - 16);
+      const int cnt = hdr[0];
+      if (cnt < 0) break;
+      const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
+      const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
+      // the segment's CF width and this lane's CF column
+      const int w = min(Wp, (recs[0].y >> 20) & 0x7ff);
+      float2 cv[Wp];
+#pragma unroll
+      for (int k = 0; k < Wp; ++k) cv[k] = k < w ? cf_s[k * Wp + jx] : make_float2(0.f, 0.f);
+      for (int l = 0; l < cnt; l += 2 * SPH) {
+        // sample u of this half: l + half + 2 u
+        int4 rr[SPH];
+        int origin[SPH];
+#pragma unroll
+        for (int u = 0; u < SPH; ++u) {
+          const int li = l + half + 2 * u;
+          rr[u] = recs[li < cnt ? li : l];
+          origin[u] = (rr[u].x & 0xffff) + Pg * ((rr[u].x >> 16) & 0xffff) + jx;
+        }
+        // SPH == 1: two partial sums (even and odd rows) for independent chains
+        constexpr int NPART = SPH == 1 ? 2 : 1;
+        float re[SPH][NPART][NPOL], im[SPH][NPART][NPOL];
+#pragma unroll
+        for (int u = 0; u < SPH; ++u)
+#pragma unroll
+          for (int q = 0; q < NPART; ++q)
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) re[u][q][p] = im[u][q][p] = 0.f;
+#pragma unroll
+        for (int k = 0; k < Wp; ++k) {
+          if (k < w) {
+            const float2 c = cv[k];
+            constexpr int Q = 0;
+#pragma unroll
+            for (int u = 0; u < SPH; ++u) {
+              const int cell = origin[u] + Pg * k;
+              const int q = NPART == 2 ? (k & 1) : Q;
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) {
+                const float2 g = g_s[p * PG2 + cell];
+                re[u][q][p] = fmaf(c.x, g.x, fmaf(c.y, g.y, re[u][q][p]));
+                im[u][q][p] = fmaf(c.y, g.x, fmaf(-c.x, g.y, im[u][q][p]));
+              }
+            }
+          }
+        }
+        float x[V];
+#pragma unroll
+        for (int u = 0; u < SPH; ++u)
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            x[2 * NPOL * u + 2 * p] = NPART == 2 ? re[u][0][p] + re[u][NPART - 1][p] : re[u][0][p];
+            x[2 * NPOL * u + 2 * p + 1] = NPART == 2 ? im[u][0][p] + im[u][NPART - 1][p] : im[u][0][p];
+          }
+        const float cr0 = half_transpose_sum<V>(x, lane);
+        const float ci0 = __shfl_down_sync(0xffffffffu, cr0, 1 << sh);
+        const int v = (lane & 15) >> sh;
+        const int u = v / (2 * NPOL);
+        const bool mine = l + half + 2 * u < cnt;
+        if (mine && (lane & ((1 << sh) - 1)) == 0 && (v & 1) == 0) {
+          const int4 r = u == 0 ? rr[0] : rr[SPH - 1];
+          const int p = (v % (2 * NPOL)) >> 1;
+          float pr = 1.f, pi = 0.f;
+          int chan = 0;
+          if (a.v.delay || a.v.mfs) {
+            const unsigned su = (unsigned)r.w, nr = (unsigned)a.v.nrow;
+            chan = (int)(su / nr);
+            phasor_of(a.v, (long long)(su - (unsigned)chan * nr), chan, &pr, &pi);
+          }
+          float cr = cr0, ci = ci0;
+          if (a.v.mfs) {
+            const float m = a.v.mfs[chan];
+            cr = __fmul_rn(cr, m);
+            ci = __fmul_rn(ci, m);
+          }
+          a.out[(size_t)r.w * NPOL + p] = make_float2(__fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi)),
+                                                      __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr)));
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[stage]);
+    }
+  }
+  __syncthreads();
+  if (s_abort && warp == ncw && lane == 0) seg_drain(nfill, NST, full);
+}
+
 // shared memory of k_degrid_t: the grid tile per polarisation, then the ring
 static size_t degrid_t_tile_bytes(int npol, int Pg) { return (size_t)npol * Pg * Pg * sizeof(float2) + 128; }
 
@@ -1840,7 +2084,7 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     pl.nitems = 0;
     return YG_OK;
   }
-  if (n >= (1ll << 31)) return YG_ERR_ARG;  // cub sizes and tile offsets are int
+  if (n >= (1ll << 31)) return YG_ERR_ARG;  // sort sizes and tile offsets are int
   YG_CUDA_TRY(pl.key.ensure(n * 8));
   YG_CUDA_TRY(pl.key_alt.ensure(n * 8));
   YG_CUDA_TRY(pl.val.ensure(n * 4));
@@ -1856,17 +2100,14 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   // radix sort over the bits that keys use (the invalid key is one past the
   // largest valid key, so it sorts last)
   const int end_bit = std::min(64, ceil_log2(a.invalid_key + 1));
-  size_t tmp = 0;
-  cub::DoubleBuffer<unsigned long long> kb(pl.key.as<unsigned long long>(), pl.key_alt.as<unsigned long long>());
-  cub::DoubleBuffer<unsigned int> vb(pl.val.as<unsigned int>(), pl.val_alt.as<unsigned int>());
-  YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, (int)n, 0, end_bit, st));
-  YG_CUDA_TRY(pl.sort_tmp.ensure(tmp));
-  YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(pl.sort_tmp.p, tmp, kb, vb, (int)n, 0, end_bit, st));
-  if (kb.Current() != pl.key.as<unsigned long long>()) {
+  YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(sort_pairs_tmp_bytes(n), scan_tmp_bytes(n))));
+  int in_alt = 0;
+  YG_CUDA_TRY(sort_pairs(pl.key.as<unsigned long long>(), pl.key_alt.as<unsigned long long>(),
+                         pl.val.as<unsigned int>(), pl.val_alt.as<unsigned int>(), n, end_bit, pl.sort_tmp.p,
+                         pl.sort_tmp.bytes, st, &in_alt));
+  if (in_alt) {
     std::swap(pl.key.p, pl.key_alt.p);
     std::swap(pl.key.bytes, pl.key_alt.bytes);
-  }
-  if (vb.Current() != pl.val.as<unsigned int>()) {
     std::swap(pl.val.p, pl.val_alt.p);
     std::swap(pl.val.bytes, pl.val_alt.bytes);
   }
@@ -1886,10 +2127,9 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   YG_COUNT_LAUNCH();
   k_count_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), nt, vmax, pl.nit.as<int>());
   YG_COUNT_LAUNCH();
-  size_t tmp2 = 0;
-  YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
-  if (tmp2 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp2));
-  YG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(pl.sort_tmp.p, tmp2, pl.nit.as<int>(), pl.itembase.as<int>(), (int)nt, st));
+  if (scan_tmp_bytes(nt) > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(scan_tmp_bytes(nt)));
+  YG_CUDA_TRY(scan_i32(pl.nit.as<int>(), pl.itembase.as<int>(), nt, SCAN_SUM, true, pl.sort_tmp.p, pl.sort_tmp.bytes,
+                       st));
   // item count and on-grid samples back to the host through mapped memory
   YG_CUDA_TRY(pl.info_h.ensure(16));
   k_plan_counts<<<1, 1, 0, st>>>(pl.itembase.as<int>() + (nt - 1), pl.nit.as<int>() + (nt - 1),
@@ -1898,25 +2138,23 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   YG_CUDA_TRY(cudaStreamSynchronize(st));
   pl.nitems = (int)pl.info_h.as<volatile long long>()[0];
   pl.nvalid = pl.info_h.as<volatile long long>()[1];
-  YG_CUDA_TRY(pl.items.ensure((size_t)std::max(1, pl.nitems) * sizeof(int4)));
+  YG_CUDA_TRY(pl.items.ensure_headroom((size_t)std::max(1, pl.nitems) * sizeof(int4)));
   k_fill_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), pl.nit.as<int>(),
                                                   pl.itembase.as<int>(), nt, vmax, pl.items.as<int4>());
   YG_COUNT_LAUNCH();
-  YG_CUDA_TRY(pl.runend.ensure((size_t)std::max(1ll, pl.nvalid) * 4));
+  YG_CUDA_TRY(pl.runend.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * 4));
   if (pl.nvalid > 0) {
     // scratch for the marks: the (now unused) alternate key buffer
     int* rev = pl.key_alt.as<int>();
     int* revmin = rev + pl.nvalid;
     k_run_marks<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), pl.nvalid, a.mbits, rev);
     YG_COUNT_LAUNCH();
-    size_t tmp3 = 0;
-    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp3, rev, revmin, cub::Min(), (int)pl.nvalid, st));
-    if (tmp3 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp3));
-    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp3, rev, revmin, cub::Min(), (int)pl.nvalid, st));
+    if (scan_tmp_bytes(pl.nvalid) > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(scan_tmp_bytes(pl.nvalid)));
+    YG_CUDA_TRY(scan_i32(rev, revmin, pl.nvalid, SCAN_MIN, false, pl.sort_tmp.p, pl.sort_tmp.bytes, st));
     k_run_unreverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(revmin, pl.nvalid, pl.runend.as<int>());
     YG_COUNT_LAUNCH();
   }
-  YG_CUDA_TRY(pl.rec.ensure((size_t)std::max(1ll, pl.nvalid) * sizeof(int4)));
+  YG_CUDA_TRY(pl.rec.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * sizeof(int4)));
   if (pl.nvalid > 0) {
     if (a.cf.wpad > 1023 || !a.cf.pad) return YG_ERR_UNSUPPORTED;  // residues are packed in 10 bits
     k_records<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.val.as<unsigned int>(), pl.pos.as<unsigned int>(),
@@ -1926,6 +2164,12 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
                                                         pl.rec.as<int4>());
     YG_COUNT_LAUNCH();
   }
+  YG_CUDA_TRY(pl.inv.ensure((size_t)n * 4));
+  YG_CUDA_TRY(cudaMemsetAsync(pl.inv.p, 0xff, (size_t)n * 4, st));
+  if (pl.nvalid > 0) {
+    k_inverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.rec.as<int4>(), pl.nvalid, pl.inv.as<int>());
+    YG_COUNT_LAUNCH();
+  }
   pl.pos_ready = false;
   if (a.pos_major && pl.nvalid > 0) {
     // a second order of the same records for gridding: tile first as before
@@ -1933,28 +2177,30 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
     // the CF index, so consecutive samples of an item mostly cover the same
     // cells (register accumulation in k_grid)
     const long long nv = pl.nvalid;
-    YG_CUDA_TRY(pl.key_alt.ensure(nv * 8));
-    YG_CUDA_TRY(pl.pos_key2.ensure(nv * 8));
-    YG_CUDA_TRY(pl.val_alt.ensure(nv * 4));
-    YG_CUDA_TRY(pl.pos_val2.ensure(nv * 4));
+    // key_alt and val_alt (free once the records are made) hold the new
+    // keys; the primary keys, read last by k_pos_keys, are the sort's
+    // alternate key buffer; only the alternate values need a buffer of
+    // their own (the primary values stay in use by the passes)
+    YG_CUDA_TRY(pl.pos_val2.ensure_headroom(nv * 4));
     k_pos_keys<<<grid_dim(nv, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), nv, a.mbits, a.cf.ncf,
                                                   a.pos_major, a.os * a.os, pl.key_alt.as<unsigned long long>(),
                                                   pl.val_alt.as<unsigned int>());
     YG_COUNT_LAUNCH();
-    cub::DoubleBuffer<unsigned long long> kb2(pl.key_alt.as<unsigned long long>(),
-                                              pl.pos_key2.as<unsigned long long>());
-    cub::DoubleBuffer<unsigned int> vb2(pl.val_alt.as<unsigned int>(), pl.pos_val2.as<unsigned int>());
-    size_t tmp4 = 0;
-    YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp4, kb2, vb2, (int)nv, 0, end_bit, st));
-    if (tmp4 > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(tmp4));
-    YG_CUDA_TRY(cub::DeviceRadixSort::SortPairs(pl.sort_tmp.p, tmp4, kb2, vb2, (int)nv, 0, end_bit, st));
-    YG_CUDA_TRY(pl.rec_pos.ensure((size_t)nv * sizeof(int4)));
-    k_permute_rec<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec.as<int4>(), vb2.Current(), nv, pl.rec_pos.as<int4>());
+    if (sort_pairs_tmp_bytes(nv) > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(sort_pairs_tmp_bytes(nv)));
+    int alt2 = 0;
+    YG_CUDA_TRY(sort_pairs(pl.key_alt.as<unsigned long long>(), pl.key.as<unsigned long long>(),
+                           pl.val_alt.as<unsigned int>(), pl.pos_val2.as<unsigned int>(), nv, end_bit,
+                           pl.sort_tmp.p, pl.sort_tmp.bytes, st, &alt2));
+    YG_CUDA_TRY(pl.rec_pos.ensure_headroom((size_t)nv * sizeof(int4)));
+    k_permute_rec<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec.as<int4>(),
+                                                     alt2 ? pl.pos_val2.as<unsigned int>() : pl.val_alt.as<unsigned int>(),
+                                                     nv, pl.rec_pos.as<int4>());
+    YG_COUNT_LAUNCH();
+    YG_CUDA_TRY(pl.inv_pos.ensure((size_t)n * 4));
+    YG_CUDA_TRY(cudaMemsetAsync(pl.inv_pos.p, 0xff, (size_t)n * 4, st));
+    k_inverse<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec_pos.as<int4>(), nv, pl.inv_pos.as<int>());
     YG_COUNT_LAUNCH();
     YG_CUDA_TRY(cudaGetLastError());
-    YG_CUDA_TRY(cudaStreamSynchronize(st));
-    pl.pos_key2.release();
-    pl.pos_val2.release();
     pl.pos_ready = true;
     pl.pos_mode = a.pos_major;
     pl.os2 = a.os * a.os;
@@ -2240,27 +2486,20 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   if (shape.threads == 0) return YG_ERR_UNSUPPORTED;
   const size_t per_item = gtile ? (size_t)v.npol * ((size_t)Pg * Pg + gtile_nthr) * sizeof(float2)
                                 : (size_t)v.npol * P * P * sizeof(float2);
-  YG_CUDA_TRY(scratch.ensure(per_item * pl.nitems));
-  YG_CUDA_TRY(svis.ensure((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
+  YG_CUDA_TRY(scratch.ensure_headroom(per_item * pl.nitems));
+  YG_CUDA_TRY(svis.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
   if (v.npol > 4) return YG_ERR_UNSUPPORTED;
-  if (pos) {
-    // visibilities in the position-major order; the sums of weights over the
-    // CF-major records, whose runs of equal rows keep the atomics few
-    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec_pos.as<int4>(), pl.nvalid, svis.as<float2>(),
-                                                           SumwArgs{nullptr, sw.chan_map, sw.os, sw.track_per_os,
-                                                                    sw.nrows, sw.nchan_img}, err);
-    YG_COUNT_LAUNCH();
-    if (sw.sumw) {
-      k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, pl.rec.as<int4>(), pl.nvalid, nullptr, sw, err);
-      YG_COUNT_LAUNCH();
-    }
-  } else {
-    // plane-major records keep the runs of equal sum-of-weights rows long
-    // (one CF plane after another in each tile): one pass does both
-    k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, planes ? pl.rec_pos.as<int4>() : pl.rec.as<int4>(),
-                                                           pl.nvalid, svis.as<float2>(), sw, err);
-    YG_COUNT_LAUNCH();
-  }
+  // the weighted visibilities in the order of the records the kernel reads,
+  // gathered in the cube's order; the weight checks and the sums of weights
+  // over the sorted records (CF-major or plane-major: runs of equal
+  // sum-of-weights rows keep the atomics few)
+  k_gather_cube<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, (pos || planes) ? pl.inv_pos.as<int>()
+                                                                               : pl.inv.as<int>(),
+                                                           svis.as<float2>());
+  YG_COUNT_LAUNCH();
+  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, planes ? pl.rec_pos.as<int4>() : pl.rec.as<int4>(),
+                                                         pl.nvalid, nullptr, sw, err);
+  YG_COUNT_LAUNCH();
   GridKArgs g;
   g.Wy = pl.wy;
   g.pos_major = pos ? 1 : 0;
@@ -2436,7 +2675,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
 // Degrids the samples of a plan from `grid` and adds the result into vis.
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf) {
+                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf, int variant) {
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
@@ -2490,10 +2729,15 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<pl.nitems, threads, smem, st>>>(d);
       };
+      // 16-wide CF planes: the register-CF kernel unless variant bit 256
+      // asks for k_degrid_t (both need a stage per tap warp)
+      const bool regcf = !learned && d.Wp == 16 && d.own && !(variant & 256);
+      // bit 512: one sample per half-warp pass instead of two
+      const bool sph1 = (variant & 512) != 0;
       switch (v.npol * 10 + (learned ? (d.ext ? 3 : 2) : 0)) {
-        case 10: launch(k_degrid_t<1, 0>); break;
-        case 20: launch(k_degrid_t<2, 0>); break;
-        case 40: launch(k_degrid_t<4, 0>); break;
+        case 10: regcf ? (sph1 ? launch(k_degrid_r<1, 1>) : launch(k_degrid_r<1, 2>)) : launch(k_degrid_t<1, 0>); break;
+        case 20: regcf ? (sph1 ? launch(k_degrid_r<2, 1>) : launch(k_degrid_r<2, 2>)) : launch(k_degrid_t<2, 0>); break;
+        case 40: regcf ? (sph1 ? launch(k_degrid_r<4, 1>) : launch(k_degrid_r<4, 2>)) : launch(k_degrid_t<4, 0>); break;
         case 12: launch(k_degrid_t<1, 2>); break;
         case 22: launch(k_degrid_t<2, 2>); break;
         case 42: launch(k_degrid_t<4, 2>); break;
@@ -2573,10 +2817,8 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
   if (!pl.prev_ready) {
     k_order_marks<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), pl.nrow, pl.nchan, 3, marks);
     YG_COUNT_LAUNCH();
-    size_t tmp = 0;
-    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(nullptr, tmp, marks, prev, cub::Max(), (int)n, st));
-    YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(tmp, pl.sort_tmp.bytes)));
-    YG_CUDA_TRY(cub::DeviceScan::InclusiveScan(pl.sort_tmp.p, tmp, marks, prev, cub::Max(), (int)n, st));
+    YG_CUDA_TRY(pl.sort_tmp.ensure(std::max(scan_tmp_bytes(n), pl.sort_tmp.bytes)));
+    YG_CUDA_TRY(scan_i32(marks, prev, n, SCAN_MAX, false, pl.sort_tmp.p, pl.sort_tmp.bytes, st));
     pl.prev_ready = true;
   }
   k_degrid_writeback<<<grid_dim(n, 256), 256, 0, st>>>(pl.status.as<unsigned char>(), prev, tmp_vals.as<float2>(),
@@ -2621,7 +2863,7 @@ __global__ void k_learned_inputs(const int4* __restrict__ rec, const unsigned lo
 int plan_learned_inputs(Plan& pl, const double* uvw, const double* freq, double cellu, double cellv, int os,
                         int nchan_img, const double* wstack, double wnorm, cudaStream_t st) {
   if (pl.ext_ready) return YG_OK;
-  YG_CUDA_TRY(pl.ext.ensure((size_t)std::max(1ll, pl.nvalid) * sizeof(float4)));
+  YG_CUDA_TRY(pl.ext.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * sizeof(float4)));
   if (pl.nvalid > 0) {
     k_learned_inputs<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(
         pl.rec.as<int4>(), pl.key.as<unsigned long long>(), pl.nvalid, uvw, freq, pl.nrow, cellu, cellv, os, pl.mbits,

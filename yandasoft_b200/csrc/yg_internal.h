@@ -37,6 +37,14 @@ struct DevBuf {
     bytes = n;
     return cudaSuccess;
   }
+  // as ensure, but a buffer that has to grow gets an eighth more than asked:
+  // sizes that vary a little from call to call (valid samples, work items of
+  // the row pieces of one chunk) then stop reallocating, and so stop the
+  // device-wide synchronisation of cudaFree between pieces
+  cudaError_t ensure_headroom(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    return ensure(n + n / 8);
+  }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
@@ -138,7 +146,8 @@ struct Plan {
   DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
   DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
   DevBuf rec_pos;               // the same records ordered by tile, then position in the tile, then CF
-  DevBuf pos_key2, pos_val2;    // sort buffers of rec_pos (released after the build)
+  DevBuf pos_val2;              // alternate values of the rec_pos sort
+  DevBuf inv, inv_pos;          // per sample id: its index in rec (rec_pos), -1 off the grid
   bool pos_ready = false;       // rec_pos is built
   int pos_mode = 0;             // its order: 1 position then CF index; 2 CF plane, position, offset
   int os2 = 1;                  // oversampling offsets per CF plane

@@ -39,7 +39,7 @@ EXPORTS = [
     "yg_set_grid_variant", "yg_degrid_noalloc", "yg_mlp_nparams", "yg_learned_train", "yg_set_cf_form",
     "yg_learned_get_params", "yg_learned_set_params", "yg_mlp_loss_grad", "yg_mlp_eval",
     "yg_cycle_create", "yg_cycle_run", "yg_cycle_info", "yg_cycle_destroy", "yg_autotune", "yg_autotune_reset",
-    "yg_cycle_create_roles",
+    "yg_cycle_create_roles", "yg_sort_pairs", "yg_scan_i32",
 ]
 
 
@@ -133,6 +133,8 @@ def load(path: str | None = None):
     L.yg_learned_set_params.argtypes = [P, P, ctypes.c_float]
     L.yg_mlp_loss_grad.argtypes = [P, P, P, I64, ctypes.c_float, P, ctypes.POINTER(D)]
     L.yg_mlp_eval.argtypes = [P, P, I64, P]
+    L.yg_sort_pairs.argtypes = [P, P, I64, I32]
+    L.yg_scan_i32.argtypes = [P, P, I64, I32, I32]
     L.yg_cycle_create.argtypes = [I32, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(yg_chunk),
                                   ctypes.POINTER(P)]
     L.yg_cycle_run.argtypes = [P, I32, ctypes.POINTER(ctypes.c_float)]
@@ -577,6 +579,26 @@ def mlp_eval(params, X):
     Y = np.zeros((X.shape[0], 2), dtype=np.float32)
     _check(load().yg_mlp_eval(p.ctypes.data, X.ctypes.data, X.shape[0], Y.ctypes.data))
     return Y
+
+
+def sort_pairs(keys, vals, end_bit=64):
+    """The plan builder's stable radix sort on host copies: (keys, vals) sorted
+    by bits [0, end_bit) of the uint64 keys, equal keys in input order."""
+    k = np.array(keys, dtype=np.uint64, copy=True)
+    v = np.array(vals, dtype=np.uint32, copy=True)
+    if k.shape != v.shape or k.ndim != 1:
+        raise ValueError("keys and vals must be 1-D arrays of one length")
+    _check(load().yg_sort_pairs(k.ctypes.data, v.ctypes.data, k.size, int(end_bit)))
+    return k, v
+
+
+def scan_i32(x, op="sum", exclusive=False):
+    """The plan builder's device scan of an int32 array (op sum, min or max)."""
+    a = np.array(x, dtype=np.int32, copy=True).reshape(-1)
+    out = np.empty_like(a)
+    _check(load().yg_scan_i32(a.ctypes.data, out.ctypes.data, a.size, {"sum": 0, "min": 1, "max": 2}[op],
+                              int(bool(exclusive))))
+    return out
 
 
 def kernel_launch_count() -> int:
