@@ -1102,8 +1102,11 @@ def run_batch(args):
         nx = w["nx"]
         acc = G.Accessor(d["uvw"], d["freq"], d["vis"], shape=(d["nrow"], d["nchan"], d["npol"]))
         gd = G.VisGridderFactory.make(ps)
-        gd.initialiseDegrid(axes, model_image(w, d["sky"], d["npol"]))
         gg = G.VisGridderFactory.make(ps)
+        if args.variant:
+            gd.set_grid_variant(args.variant)
+            gg.set_grid_variant(args.variant)
+        gd.initialiseDegrid(axes, model_image(w, d["sky"], d["npol"]))
         gg.initialiseGrid(axes, (nx, nx, d["npol"], 1))
         insts.append(d)
         dgs.append(gd)

@@ -115,4 +115,13 @@ __device__ inline void raise_error(DevError* e, int code, long long where) {
   if (atomicCAS(&e->code, 0, code) == 0) e->where = where;
 }
 
+// Where-field of a bounded wait that gave up (YG_ERR_TIMEOUT): the kernel
+// (1 k_grid, 2 k_grid_pl, 3 k_degrid_t, 4 k_degrid_r), the waiting role (1 the
+// producer warp for a free stage, 2 a tap warp for a filled one, 3 the
+// producer for the plane buffer), the segment index and the block.
+__device__ inline long long timeout_where(int kernel, int role, int seg, int block) {
+  return ((long long)kernel << 60) | ((long long)role << 56) | ((long long)(seg & 0xffffff) << 32) |
+         (long long)(unsigned)block;
+}
+
 }  // namespace yg

@@ -446,6 +446,17 @@ void Gridder::check_error(cudaStream_t st) {
       case YG_ERR_WRANGE: m = "W scaling error: recommend allowing larger range of w"; break;
       case YG_ERR_WEIGHT: m = "Weight is supposed to be a positive number"; break;
       case YG_ERR_CINDEX: m = "Index into convolution functions exceeds number of planes"; break;
+      case YG_ERR_TIMEOUT: {
+        // timeout_where(): kernel, waiting role, segment, block
+        static const char* kern[] = {"?", "k_grid", "k_grid_pl", "k_degrid_t", "k_degrid_r"};
+        static const char* role[] = {"?", "producer waiting for a free stage", "tap warp waiting for a filled stage",
+                                     "producer waiting for the plane buffer"};
+        const unsigned long long w = (unsigned long long)h.where;
+        const int k = (int)(w >> 60) & 7, r = (int)(w >> 56) & 15;
+        throw YgError{h.code, std::string("a bounded wait gave up in ") + kern[k < 5 ? k : 0] + " (" +
+                                  role[r < 4 ? r : 0] + ", segment " + std::to_string((w >> 32) & 0xffffff) +
+                                  ", block " + std::to_string(w & 0xffffffffull) + ")"};
+      }
       default: m = "device error"; break;
     }
     throw YgError{h.code, m + " (sample " + std::to_string(h.where) + ")"};
@@ -849,7 +860,7 @@ std::vector<uint8_t> Gridder::psf_rows(const Chunk& c) {
   return ok;
 }
 
-void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st) {
+void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st, bool for_grid) {
   if (!st) st = stream_;
   throw_if(dc.npol != npol_, YG_ERR_UNSUPPORTED,
            "visibility and image polarisation frames must match (no polarisation conversion)");
@@ -871,6 +882,7 @@ void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st) {
   }
   BinArgs a;
   fill_bin_args(a, dc, pl.chanmap.as<int>(), row_ok);
+  if (!for_grid) a.pos_major = 0;
   // samples per work item: enough items for ~8 per SM, never below 512
   int vmax = vmax_;
   TuneChoice tc;
@@ -986,7 +998,7 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
     cuda_check(cudaStreamWaitEvent(bin_stream_, piece_up_[b], 0), "wait upload");
     cuda_check(cudaStreamWaitEvent(bin_stream_, piece_pass_[b], 0), "wait pass");
     init_cf(staged[b]);
-    bin(staged[b], piece_plan_[b], bin_stream_);
+    bin(staged[b], piece_plan_[b], bin_stream_, !degridding);
     cuda_check(cudaEventRecord(piece_binned_, bin_stream_), "event");
   };
   // no pass has used the buffers yet: their pass events complete at once
@@ -1128,7 +1140,7 @@ void Gridder::degrid(Chunk& c) {
   if (!c.on_device) dc.pointing = c.pointing;
   init_cf(dc);
   Plan& pl = plan_;
-  bin(dc, pl);
+  bin(dc, pl, nullptr, false);
   degrid_plan(dc, pl);
   if (!c.on_device) {
     const size_t bytes = (size_t)c.nrow * c.nchan * c.npol * sizeof(float2);
@@ -1139,12 +1151,12 @@ void Gridder::degrid(Chunk& c) {
 
 // The kernels of one degrid pass over a plan on st (see grid_enqueue).
 void Gridder::degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0,
-                             cudaEvent_t k1) {
+                             cudaEvent_t k1, bool alone) {
   VisArgs v = vis_args(dc, mfs, false);
   const LearnedCF lcf = learned_view_for(dc, pl);
   rc_check(plan_degrid(pl, v, dc.vis, cf_.view(), grids_.as<float2>(), nx_, ny_, nchan_, pl.chanmap.as<int>(), tmpvals_,
                        carry_.as<float2>(), err_.as<DevError>(), st, k0, k1, cf_form_ != 0 ? &lcf : nullptr,
-                       grid_variant()),
+                       grid_variant(), alone),
            "degridding");
 }
 

@@ -129,15 +129,18 @@ class Gridder {
   float2* device_grid() { return grids_.as<float2>(); }
   cudaStream_t stream() const { return stream_; }
   // plan-level API for repeated passes over the same data
-  void bin(const Chunk& c, Plan& pl, cudaStream_t st = nullptr);
+  // for_grid false: a plan for degridding only (no second, gridding record order)
+  void bin(const Chunk& c, Plan& pl, cudaStream_t st = nullptr, bool for_grid = true);
   void grid_plan(const Chunk& c, const Plan& pl);
   void degrid_plan(Chunk& c, Plan& pl);
   // launch-only cores of grid_plan / degrid_plan: no host synchronisation,
   // no allocation once sized, any stream (what a CUDA graph records)
   void grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
                     cudaEvent_t k1 = nullptr);
+  // alone = false where other instances' passes share the GPU (the major-cycle
+  // graph): the degrid kernels then use their all-warps ring protocol
   void degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
-                      cudaEvent_t k1 = nullptr);
+                      cudaEvent_t k1 = nullptr, bool alone = true);
   const float* mfs_weights(const Chunk& dc);
   TuneReport autotune(const Chunk& dc, int max_trials);
   void apply_tuning(const TuneChoice& c) {

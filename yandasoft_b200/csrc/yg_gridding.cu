@@ -248,7 +248,10 @@ struct GridKArgs {
 
 constexpr int kGridThreads = 256;
 constexpr int kBatch = 64;
-constexpr long long kWaitLimit = 1ll << 22;   // bounded mbarrier waits
+// bounded mbarrier waits: a wait gives up after 4 s on the global timer (and
+// after 2^26 polls, should the timer not advance)
+constexpr unsigned long long kWaitNs = 4000000000ull;
+constexpr long long kWaitPolls = 1ll << 26;
 
 struct VisRec {
   int cb;            // footprint origin cell (px0 + P py0) in the padded tile
@@ -288,10 +291,33 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// bounded wait; false when the limit was reached
+// try_wait that may suspend the thread up to hint_ns while the phase is open
+__device__ __forceinline__ bool mbar_try_wait_for(unsigned long long* bar, unsigned phase, unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait; false when the limit was reached.  The bound is time, not a
+// poll count: CTAs of many kernels sharing the SMs (the major-cycle graph runs
+// instances side by side) can make an ordinary wait last many polls.
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
-  for (long long i = 0; i < kWaitLimit; ++i)
-    if (mbar_try_wait(bar, phase)) return true;
+  if (mbar_try_wait(bar, phase)) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long i = 0; i < kWaitPolls; ++i) {
+    if (mbar_try_wait_for(bar, phase, 100000u)) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
+  }
   return false;
 }
 
@@ -555,7 +581,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
                            empty, nfill, CFS, CFM == 3 ? a.ext : nullptr, 1, CFS ? a.pps : 1, a.cfplane,
                            CFM != 1)) {
       if (lane == 0) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(1, 1, nfill, blockIdx.x));
         s_abort = 1;
       }
     }
@@ -599,7 +625,7 @@ __global__ void __launch_bounds__(CFM >= 2 ? 288 : 544) k_grid(GridKArgs a) {
     for (int nseg_done = 0;; ++nseg_done) {
       const int stage = nseg_done % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg_done / NST) & 1u)) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(1, 2, nseg_done, blockIdx.x));
         s_abort = 1;
         break;
       }
@@ -866,7 +892,7 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     // ---- producer
     const unsigned fm = 0xffffffffu;
     const unsigned rowbytes = (unsigned)prow * sizeof(float2);
-    int seg = 0, cur_plane = -1;
+    int seg = 0, cur_plane = -1, why = 1;
     bool ok = true;
     auto load = [&](int base, int4& r, float2 (&v)[NPOL]) {
       const int i = base + lane;
@@ -932,7 +958,11 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
                          &full[stage]);
             }
           }
-          if (!__shfl_sync(fm, okp ? 1 : 0, 0)) { ok = false; break; }
+          if (!__shfl_sync(fm, okp ? 1 : 0, 0)) {
+            ok = false;
+            why = 3;
+            break;
+          }
           cur_plane = plane;
         } else if (lane == 0) {
           mbar_arrive(&full[stage]);
@@ -957,7 +987,7 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     }
     nfill = seg;
     if (!ok && lane == 0) {
-      raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+      raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(2, why, seg, blockIdx.x));
       s_abort = 1;
     }
   } else {
@@ -982,7 +1012,7 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     for (int nseg = 0;; ++nseg) {
       const int stage = nseg % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(2, 2, nseg, blockIdx.x));
         s_abort = 1;
         break;
       }
@@ -1545,9 +1575,9 @@ struct DegridTArgs {
 // With a.own (not in CFM 2, whose planes the warps evaluate together, and only
 // with at least one stage per tap warp), segment s belongs to tap warp
 // s mod ncw, which alone waits for it, degrids all its samples and releases
-// its stage (empty barriers of count 1): warps do not touch the barriers of
-// segments that are not theirs.  Otherwise every warp walks every segment and
-// takes the samples whose index in the item is its own modulo ncw.
+// its stage (empty barriers of count 1).  Otherwise every warp walks every
+// segment and takes the samples whose index in the item is its own modulo
+// ncw (empty barriers of count ncw).
 template <int NPOL, int CFM>
 __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
   const bool OWN = CFM != 2 && a.own;
@@ -1599,7 +1629,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
     if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp2, a.cfbuf, SB, NST, ring, full, empty, nfill,
                         CFM == 0, CFM == 3 ? a.ext : nullptr, OWN ? ncw : 1)) {
       if (lane == 0) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(3, 1, nfill, blockIdx.x));
         s_abort = 1;
       }
     }
@@ -1612,7 +1642,7 @@ __global__ void __launch_bounds__(288) k_degrid_t(DegridTArgs a) {
     for (int nseg = OWN ? warp : 0;; nseg += OWN ? ncw : 1) {
       const int stage = nseg % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(3, 2, nseg, blockIdx.x));
         s_abort = 1;
         break;
       }
@@ -1747,9 +1777,12 @@ __device__ __forceinline__ float half_transpose_sum(float (&x)[V], int lane) {
 
 // GridKernel::degrid (GridKernel.cc:99-137) for 16-wide CF planes without the
 // learned CF: k_degrid_t's item, tile and segment ring, with the tap warps
-// working differently.  Each warp owns every ncw-th segment (one CF plane,
-// up to kSeg samples) and takes its samples two at a time, one per
-// half-warp: lane jx = lane & 15 of a half walks the rows of its sample's
+// working differently.  Warp s mod ncw degrids segment s (one CF plane, up to
+// kSeg samples); with a.own it alone waits for and releases the segment (the
+// ring protocol of k_degrid_t's owned segments), otherwise every tap warp
+// waits for every segment and releases it, passing over the others' (empty
+// barriers of count ncw, one terminal segment).  A warp takes its segment's
+// samples two at a time, one per half-warp: lane jx = lane & 15 of a half walks the rows of its sample's
 // footprint (one 16-wide grid row per half-warp load, which is one
 // shared-memory wavefront per 64-bit load), and keeps the column jx of the
 // segment's CF plane, rows 0..w-1, in registers, read once per segment rather
@@ -1785,7 +1818,7 @@ __global__ void __launch_bounds__(288) k_degrid_r(DegridTArgs a) {
     s_abort = 0;
     for (int q = 0; q < NST; ++q) {
       mbar_init(&full[q], 1);
-      mbar_init(&empty[q], 1);
+      mbar_init(&empty[q], a.own ? 1 : ncw);
     }
     mbar_fence_init();
   }
@@ -1801,9 +1834,9 @@ __global__ void __launch_bounds__(288) k_degrid_r(DegridTArgs a) {
   int nfill = 0;
   if (warp == ncw) {
     if (!seg_produce<0>(it, a.rec, nullptr, 0, 0, a.cf.pad, Wp * Wp, a.cfbuf, SB, NST, ring, full, empty, nfill,
-                        true, nullptr, ncw)) {
+                        true, nullptr, a.own ? ncw : 1)) {
       if (lane == 0) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(4, 1, nfill, blockIdx.x));
         s_abort = 1;
       }
     }
@@ -1811,10 +1844,10 @@ __global__ void __launch_bounds__(288) k_degrid_r(DegridTArgs a) {
     const int jx = lane & 15, half = lane >> 4;
     constexpr int V = 2 * NPOL * SPH;
     constexpr int sh = V == 16 ? 0 : (V == 8 ? 1 : (V == 4 ? 2 : 3));   // 4 - log2(V)
-    for (int nseg = warp;; nseg += ncw) {
+    for (int nseg = a.own ? warp : 0;; nseg += a.own ? ncw : 1) {
       const int stage = nseg % NST;
       if (!mbar_wait(&full[stage], (unsigned)(nseg / NST) & 1u)) {
-        raise_error(a.err, YG_ERR_TIMEOUT, blockIdx.x);
+        raise_error(a.err, YG_ERR_TIMEOUT, timeout_where(4, 2, nseg, blockIdx.x));
         s_abort = 1;
         break;
       }
@@ -1822,6 +1855,12 @@ __global__ void __launch_bounds__(288) k_degrid_r(DegridTArgs a) {
       const volatile int* hdr = reinterpret_cast<const volatile int*>(sp + SB - 16);
       const int cnt = hdr[0];
       if (cnt < 0) break;
+      if (!a.own && nseg % ncw != warp) {
+        // another warp's segment: pass it
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        continue;
+      }
       const float2* __restrict__ cf_s = reinterpret_cast<const float2*>(sp);
       const int4* recs = reinterpret_cast<const int4*>(sp + a.cfbuf);
       // the segment's CF width and this lane's CF column
@@ -1914,8 +1953,8 @@ size_t degrid_t_smem_bytes(int npol, int Pg, int cfbuf, int nst) {
   return degrid_t_tile_bytes(npol, Pg) + (size_t)nst * (seg_stage_bytes(cfbuf, 0) + 16);
 }
 
-// Ring depth of k_degrid_t: up to 16 stages (two per tap warp, each warp
-// owning every eighth segment), as many as fit with two CTAs per SM when at
+// Ring depth of k_degrid_t and k_degrid_r: up to 16 stages (two per tap
+// warp), as many as fit with two CTAs per SM when at
 // least min_stages_two_ctas do, else as many as fit one CTA; 0 when not even 2
 // fit.
 int degrid_t_stages(int npol, int Pg, int cfbuf) {
@@ -2675,7 +2714,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
 // Degrids the samples of a plan from `grid` and adds the result into vis.
 int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, const float2* grid, int nx, int ny,
                 int nchan_img, const int* chan_map, DevBuf& tmp_vals, float2* carry, DevError* err,
-                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf, int variant) {
+                cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf, int variant, bool alone) {
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
@@ -2721,7 +2760,10 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
       smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
     }
     d.stage_bytes = seg_stage_bytes(d.cfbuf, xv);
-    d.own = d.nstages >= kDegridThreads / 32 ? 1 : 0;
+    // owned segments (the faster protocol) where this pass is the only ring
+    // kernel running; the all-warps protocol where instances share the GPU
+    // (owned segments timed out there)
+    d.own = (alone && d.nstages >= kDegridThreads / 32) ? 1 : 0;
     if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
       const int threads = kDegridThreads + 32;   // tap warps + the producer warp
@@ -2731,7 +2773,7 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
       };
       // 16-wide CF planes: the register-CF kernel unless variant bit 256
       // asks for k_degrid_t (both need a stage per tap warp)
-      const bool regcf = !learned && d.Wp == 16 && d.own && !(variant & 256);
+      const bool regcf = !learned && d.Wp == 16 && d.nstages >= kDegridThreads / 32 && !(variant & 256);
       // bit 512: one sample per half-warp pass instead of two
       const bool sph1 = (variant & 512) != 0;
       switch (v.npol * 10 + (learned ? (d.ext ? 3 : 2) : 0)) {
