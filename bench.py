@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity leg (1% row subset against the oracle)")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the track (tests only)")
+    ap.add_argument("--grid-nx", type=int, default=0,
+                    help="grid side override with --cell-arcsec (small profiling cases: 2048 at 8 arcsec keeps "
+                         "config 1's field and CF support at a quarter of the grid memory)")
+    ap.add_argument("--cell-arcsec", type=float, default=0.0, help="cell override (see --grid-nx)")
     ap.add_argument("--tile", type=int, default=0, help="uv tile side (0 = automatic)")
     ap.add_argument("--variant", type=int, default=0, help="k_grid thread layout variant (0 = automatic)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-CF leg")
@@ -519,8 +523,19 @@ def torch_index(a):
 # --------------------------------------------------------------------------
 # arms
 # --------------------------------------------------------------------------
-def roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak, peak_kind, sm_hz, cf_bytes):
-    """Roofline of the dominant kernel (k_grid) and of k_degrid_t, per launch
+def kernel_names(variant, support):
+    """The grid and degrid kernels a pass runs for a k_grid variant: the
+    plane-major k_grid_pl with variant bit 64, else k_grid; k_degrid_r for
+    16-wide CFs unless variant bit 256 asks for k_degrid_t."""
+    v = variant or 1
+    grid = "k_grid_pl" if v & 64 else "k_grid"
+    degrid = "k_degrid_r" if (2 * support + 1 <= 16 and not v & 256) else "k_degrid_t"
+    return grid, degrid
+
+
+def roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak, peak_kind, sm_hz, cf_bytes,
+             names=("k_grid", "k_degrid_t")):
+    """Roofline of the dominant kernel (the grid pass's) and of the degrid kernel, per launch
     (one grid or degrid pass over the workload).  The binding roofline time is
     t_roof = max(algorithmic HBM bytes / measured HBM bandwidth,
     8 flops per tap x taps / FP32 peak at the sampled SM clock); frac =
@@ -556,27 +571,38 @@ def roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak,
 
     g = one(kgrid_ms, hbm_grid, 16.0 * npol + 8.0)
     dg = one(kdeg_ms, hbm_degrid, 8.0 * npol + 8.0)
-    traffic = kgrid_traffic(info, support, npol)
-    return {"bound": g["bound"], "kernel": "k_grid", "achieved": g["fp32"]["achieved_tflops"],
+    traffic = kgrid_traffic(info, support, npol, names[0])
+    return {"bound": g["bound"], "kernel": names[0], "achieved": g["fp32"]["achieved_tflops"],
             "peak": g["fp32"]["peak_tflops"], "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 flops) at the "
                                                            "sampled SM clock",
             "unit": "TFLOP/s", "frac": g["frac"], "traffic": traffic,
-            "traffic_note": "DRAM bytes per k_grid launch, scaled from a single-kernel ncu capture of a small slice "
-                            "of this workload by samples and work items",
+            "traffic_note": "DRAM bytes per %s launch, scaled from a single-kernel ncu capture of a small case "
+                            "of this workload by samples and work items" % names[0],
             "t_roof_ms": g["t_roof_ms"], "kgrid_ms": round(kgrid_ms, 4), "kdegrid_ms": round(kdeg_ms, 4),
-            "k_grid": g, "k_degrid_t": dg, "taps_per_s": round(taps * nvalid_vis / (kgrid_ms / 1e3), 1)
+            names[0]: g, names[1]: dg, "taps_per_s": round(taps * nvalid_vis / (kgrid_ms / 1e3), 1)
             if kgrid_ms > 0 else 0,
             "note": "t_roof = max(algorithmic HBM bytes / measured HBM bandwidth, 8 flops x taps / FP32 peak); "
                     "frac = t_roof / kernel time; smem frac: the named shared-memory bytes per tap and sample "
                     "over 128 B per clock per SM"}
 
 
-def kgrid_traffic(info, support, npol):
-    """DRAM bytes of one k_grid launch, from the per-sample and per-item rates
-    of an ncu capture of a slice of the same workload: the sorted records and
-    visibilities read per sample, the padded tiles written per item."""
+# DRAM bytes of one grid launch per on-grid sample and per work item x
+# polarisation x padded-tile cell, from single-kernel ncu captures of a small
+# case of config 1 (k_grid: the sorted records and visibilities read per
+# sample, the padded tiles written per item)
+# (k_grid_pl: records and the cube's visibility sectors read per sample, the
+# item's global tile reduced and read back per cell)
+TRAFFIC_RATES = {"k_grid": (48.9, 0.84 * 8), "k_grid_pl": (303.0, 26.6)}
+
+
+def kgrid_traffic(info, support, npol, name="k_grid"):
+    """DRAM bytes of one grid launch from the kernel's captured rates (None
+    when no capture of the kernel gives them)."""
+    if name not in TRAFFIC_RATES:
+        return None
+    per_sample, per_cell = TRAFFIC_RATES[name]
     pad = info["tile"] + 2 * support
-    return int(48.9 * info["nvalid"] + 0.84 * info["nitems"] * npol * pad * pad * 8)
+    return int(per_sample * info["nvalid"] + per_cell * info["nitems"] * npol * pad * pad)
 
 
 def run_b200(args, w):
@@ -669,8 +695,9 @@ def run_b200(args, w):
     taps = (2 * support + 1) ** 2
     hbm_peak, peak_kind = peaks()
     sm_hz = (clk.summary().get("sm_mhz") or 1965.0) * 1e6
+    variant = args.variant or ((tune or {}).get("variant") or 0)
     roof = roofline(w, d, info, support, npol, nvalid_vis, kgrid_ms, kdeg_ms, hbm_peak, peak_kind, sm_hz,
-                    gg.cf_bytes())
+                    gg.cf_bytes(), kernel_names(variant, support))
     line = {
         "metric": METRIC,
         "cf_form": "plain (tabulated CF)",
@@ -1360,6 +1387,8 @@ def main():
         run_batch(args)
         return
     w = workload(args.config, args.scale)
+    if args.grid_nx:
+        w.update(nx=args.grid_nx, cell=args.cell_arcsec or w["cell"])
     if args.impl == "reference":
         run_reference(args, w)
     elif args.config == 2:

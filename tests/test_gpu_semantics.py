@@ -413,8 +413,11 @@ def test_preconditioner_function_gridder(ygmod, oracle_mod, kind, npol):
         gd.degrid(Accessor(ds.uvw, ds.freq, np.zeros_like(ds.vis)))
 
 
-@pytest.mark.parametrize("variant,pcf", [(65, False), (65, True), (66, False), (67, True), (193, False), (194, True), (49, False), (17, False)])
-def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
+@pytest.mark.parametrize("variant,pcf,direct", [(65, False, False), (65, True, False), (66, False, False),
+                                                (67, True, False), (193, False, False), (194, True, False),
+                                                (49, False, False), (17, False, False), (193, False, True),
+                                                (65, True, True)])
+def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf, direct):
     """The k_grid variants the autotuner may pick, each against the oracle on
     flagged, weighted, phase-rotated data with 4 polarisations: 65 (records in
     plane-major order, each CF plane's oversampling offsets staged in shared
@@ -423,7 +426,9 @@ def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
     with the tile in global memory, reductions at each flush), 49
     (position-major records, taps through L2) and 17 (register accumulation
     over the CF-major records).  Grids 1e-5, sums of weights exact; the
-    preconditioner's conjugate half through the plane-major kernel."""
+    preconditioner's conjugate half through the plane-major kernel.  direct:
+    through grid() itself, whose plan serves gridding only and, for the
+    plane-major kernel, is sorted once by the plane-major key."""
     from yandasoft_b200.gridder import Accessor, Axes
     import oracle
     ds = _data(npol=4, nchan=4, seed=61, duration=300.0)
@@ -435,8 +440,11 @@ def test_grid_record_orders_against_oracle(ygmod, oracle_mod, variant, pcf):
     gg.set_grid_variant(variant)
     gg.initialiseGrid(Axes(cell, cell), (nx, nx, 4, 1), dopcf=pcf)
     acc = Accessor(ds.uvw, ds.freq, ds.vis, noise=noise, flag=flag, delay=delay).to_device()
-    plan = gg.plan(acc)
-    gg.grid_plan(plan, acc)
+    if direct:
+        gg.grid(acc)
+    else:
+        plan = gg.plan(acc)
+        gg.grid_plan(plan, acc)
     og.initialise_grid(nx, nx, 4, 1, cell, cell, dopcf=pcf)
     og.grid(oracle.Chunk(uvw=ds.uvw, freq=ds.freq, vis=ds.vis, noise=noise, flag=flag, delay=delay))
     assert gg.support()[0] == og.cache.support <= 7

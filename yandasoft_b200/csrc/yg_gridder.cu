@@ -817,6 +817,8 @@ void Gridder::fill_bin_args(BinArgs& a, const Chunk& dc, const int* dchan_map, c
   // (the plane-major kernel keeps exact rows with every layout)
   a.wy = (wpad16 == 16 && ((grid_variant() & 15) <= 1 || (grid_variant() & 64)) && exact_rows_) ? 2 * smax + 1 : 0;
   a.pos_major = (grid_variant() & 64) ? 2 : ((grid_variant() & 32) ? 1 : 0);
+  a.key_planes = 0;
+  a.need_inv = 1;
   a.ntx = (nx_ + a.tile - 1) / a.tile;
   a.nty = (ny_ + a.tile - 1) / a.tile;
   int mb = 0;
@@ -860,7 +862,7 @@ std::vector<uint8_t> Gridder::psf_rows(const Chunk& c) {
   return ok;
 }
 
-void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st, bool for_grid) {
+void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st, int use) {
   if (!st) st = stream_;
   throw_if(dc.npol != npol_, YG_ERR_UNSUPPORTED,
            "visibility and image polarisation frames must match (no polarisation conversion)");
@@ -882,7 +884,14 @@ void Gridder::bin(const Chunk& dc, Plan& pl, cudaStream_t st, bool for_grid) {
   }
   BinArgs a;
   fill_bin_args(a, dc, pl.chanmap.as<int>(), row_ok);
-  if (!for_grid) a.pos_major = 0;
+  if (use == PLAN_DEGRID) a.pos_major = 0;
+  // a gridding-only plan for the plane-major kernel sorts once, by its key
+  const int wpad_b = ((cf_.maxsize + 15) / 16) * 16;
+  a.key_planes = (use == PLAN_GRID && a.pos_major == 2 && wpad_b == 16 && a.wy > 0 && a.wy <= 16 &&
+                  !cf_.view().varsup && dc.npol <= 4 && cf_form_ == 0)
+                     ? 1
+                     : 0;
+  a.need_inv = (use != PLAN_DEGRID && !a.key_planes) ? 1 : 0;
   // samples per work item: enough items for ~8 per SM, never below 512
   int vmax = vmax_;
   TuneChoice tc;
@@ -998,7 +1007,7 @@ void Gridder::run_pieces(Chunk& c, bool degridding) {
     cuda_check(cudaStreamWaitEvent(bin_stream_, piece_up_[b], 0), "wait upload");
     cuda_check(cudaStreamWaitEvent(bin_stream_, piece_pass_[b], 0), "wait pass");
     init_cf(staged[b]);
-    bin(staged[b], piece_plan_[b], bin_stream_, !degridding);
+    bin(staged[b], piece_plan_[b], bin_stream_, degridding ? PLAN_DEGRID : PLAN_GRID);
     cuda_check(cudaEventRecord(piece_binned_, bin_stream_), "event");
   };
   // no pass has used the buffers yet: their pass events complete at once
@@ -1052,7 +1061,7 @@ void Gridder::grid(const Chunk& c) {
   if (!c.on_device) dc.pointing = c.pointing;
   init_cf(dc);
   Plan& pl = plan_;
-  bin(dc, pl);
+  bin(dc, pl, nullptr, PLAN_GRID);
   grid_plan(dc, pl);
 }
 
@@ -1140,7 +1149,7 @@ void Gridder::degrid(Chunk& c) {
   if (!c.on_device) dc.pointing = c.pointing;
   init_cf(dc);
   Plan& pl = plan_;
-  bin(dc, pl, nullptr, false);
+  bin(dc, pl, nullptr, PLAN_DEGRID);
   degrid_plan(dc, pl);
   if (!c.on_device) {
     const size_t bytes = (size_t)c.nrow * c.nchan * c.npol * sizeof(float2);

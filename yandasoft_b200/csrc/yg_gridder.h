@@ -129,8 +129,10 @@ class Gridder {
   float2* device_grid() { return grids_.as<float2>(); }
   cudaStream_t stream() const { return stream_; }
   // plan-level API for repeated passes over the same data
-  // for_grid false: a plan for degridding only (no second, gridding record order)
-  void bin(const Chunk& c, Plan& pl, cudaStream_t st = nullptr, bool for_grid = true);
+  // what a plan serves: both passes; gridding only (with the plane-major
+  // kernel: one sort, by its key); degridding only (no gridding record order)
+  enum PlanUse { PLAN_BOTH = 0, PLAN_GRID = 1, PLAN_DEGRID = 2 };
+  void bin(const Chunk& c, Plan& pl, cudaStream_t st = nullptr, int use = PLAN_BOTH);
   void grid_plan(const Chunk& c, const Plan& pl);
   void degrid_plan(Chunk& c, Plan& pl);
   // launch-only cores of grid_plan / degrid_plan: no host synchronisation,

@@ -133,8 +133,16 @@ __global__ void k_bin(BinArgs a, unsigned long long* __restrict__ key, unsigned 
                 const long long tile = tx + (long long)a.ntx * ty;
                 const long long gc = (long long)gind * a.nchan_img + ichan;
                 const unsigned int m = morton2((unsigned)(iuo - tx * a.tile), (unsigned)(ivo - ty * a.tile));
-                k = (((unsigned long long)(gc * ntiles + tile) * (unsigned long long)a.cf.ncf + (unsigned)cfi)
-                     << a.mbits) | m;
+                if (a.key_planes) {
+                  // plane-major: tile, CF plane, position, oversampling offset
+                  const unsigned long long os2 = (unsigned long long)a.os * a.os;
+                  const unsigned long long cp = (unsigned)cfi / os2, fr = (unsigned)cfi % os2;
+                  k = (((((unsigned long long)(gc * ntiles + tile) * ((unsigned long long)a.cf.ncf / os2) + cp)
+                         << a.mbits) | m) * os2) + fr;
+                } else {
+                  k = (((unsigned long long)(gc * ntiles + tile) * (unsigned long long)a.cf.ncf + (unsigned)cfi)
+                       << a.mbits) | m;
+                }
                 p = (unsigned)iuo | ((unsigned)ivo << 16);
               } else {
                 st = 2;
@@ -152,21 +160,23 @@ __global__ void k_bin(BinArgs a, unsigned long long* __restrict__ key, unsigned 
   }
 }
 
-// tile id of a sorted key
-__device__ __forceinline__ long long key_tile(unsigned long long k, int mbits, int ncf) {
-  return (long long)((k >> mbits) / (unsigned long long)ncf);
+// tile id of a sorted key: ((tile * ncf + cfi) << mbits) | morton, or with
+// kos2 = os^2 the plane-major key of a gridding-only plan,
+// ((((tile * ncp + plane) << mbits) | morton) * os^2 + offset), ncp = ncf / os^2
+__device__ __forceinline__ long long key_tile(unsigned long long k, int mbits, int ncf, int kos2) {
+  return (long long)(((k / (unsigned long long)kos2) >> mbits) / (unsigned long long)(ncf / kos2));
 }
 
-__global__ void k_tile_bounds(const unsigned long long* __restrict__ key, long long n, int mbits, int ncf,
+__global__ void k_tile_bounds(const unsigned long long* __restrict__ key, long long n, int mbits, int ncf, int kos2,
                               unsigned long long invalid_key, int* __restrict__ tstart, int* __restrict__ tend,
                               long long* nvalid) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const unsigned long long k = key[i];
     if (k >= invalid_key) continue;
-    const long long t = key_tile(k, mbits, ncf);
-    if (i == 0 || key_tile(key[i - 1], mbits, ncf) != t) tstart[t] = (int)i;
+    const long long t = key_tile(k, mbits, ncf, kos2);
+    if (i == 0 || key_tile(key[i - 1], mbits, ncf, kos2) != t) tstart[t] = (int)i;
     const bool last = (i == n - 1) || key[i + 1] >= invalid_key;
-    if (last || key_tile(key[i + 1], mbits, ncf) != t) tend[t] = (int)(i + 1);
+    if (last || key_tile(key[i + 1], mbits, ncf, kos2) != t) tend[t] = (int)(i + 1);
     if (last) *nvalid = i + 1;
   }
 }
@@ -212,6 +222,25 @@ __device__ __forceinline__ void phasor_of(const VisArgs& v, long long row, int c
   *pi = (float)sin(ph);
 }
 
+// rVis = phasor * conj(vis) * wt (* mfs) of sample s, polarisation p
+// (TableVisGridder.cc:775-806), wt (* mfs) for the PSF, wt for the
+// preconditioner function; FP32 with explicit rounding.
+__device__ __forceinline__ float2 weighted_vis(const VisArgs& v, long long s, long long n, int p, float pr, float pi,
+                                               float m) {
+  const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
+  const float wt = noise_weight(nre);
+  if (v.pcf) return make_float2(__fmul_rn(1.f, wt), __fmul_rn(0.f, wt));
+  if (v.psf) return make_float2(__fmul_rn(__fmul_rn(1.f, wt), m), __fmul_rn(__fmul_rn(0.f, wt), m));
+  const float2 vv = v.vis[s + n * p];
+  const float vr = vv.x, vi = -vv.y;
+  float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
+  float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
+  rr = __fmul_rn(__fmul_rn(rr, wt), m);
+  ri = __fmul_rn(__fmul_rn(ri, wt), m);
+  return make_float2(rr, ri);
+}
+
+
 // ---------------------------------------------------------------------------
 // k_grid
 // ---------------------------------------------------------------------------
@@ -219,8 +248,8 @@ struct GridKArgs {
   const int4* items;
   const unsigned int* val;   // sample ids, sorted
   const int4* rec;           // per sorted sample: cell, residues|w, cf index, sample id
-  const float2* svis;        // per sorted sample: npol weighted visibilities
-  const int* runend;         // per sorted index at a run start: end of its run
+  const float2* svis;        // per sorted sample: npol weighted visibilities (k_grid_pl: null,
+                             // its producer forms them from the cube itself)
   const unsigned int* pos;   // iu | iv << 16, unsorted (by sample id)
   const int* cfi;            // unsorted
   VisArgs v;
@@ -894,12 +923,25 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
     const unsigned rowbytes = (unsigned)prow * sizeof(float2);
     int seg = 0, cur_plane = -1, why = 1;
     bool ok = true;
+    const long long ncube = a.v.nrow * (long long)a.v.nchan;
     auto load = [&](int base, int4& r, float2 (&v)[NPOL]) {
       const int i = base + lane;
       if (i < it.z) {
         r = a.rec[i];
+        if (a.svis) {
 #pragma unroll
-        for (int p = 0; p < NPOL; ++p) v[p] = a.svis[(size_t)i * a.npol_total + a.pol0 + p];
+          for (int p = 0; p < NPOL; ++p) v[p] = a.svis[(size_t)i * a.npol_total + a.pol0 + p];
+        } else {
+          // the weighted visibilities straight from the cube (random 8-byte
+          // reads, a window ahead of their use, beside a compute-bound kernel)
+          const unsigned nr32 = (unsigned)a.v.nrow;
+          const int chan = (int)((unsigned)r.w / nr32);
+          float pr = 1.f, pi = 0.f;
+          if (!a.v.psf && !a.v.pcf) phasor_of(a.v, (long long)((unsigned)r.w - (unsigned)chan * nr32), chan, &pr, &pi);
+          const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) v[p] = weighted_vis(a.v, r.w, ncube, a.pol0 + p, pr, pi, m);
+        }
       } else {
         r = make_int4(0, 0, -1, -1);
       }
@@ -1117,7 +1159,7 @@ __global__ void __launch_bounds__(544) k_grid_pl(GridKArgs a) {
 // (TableVisGridder.cc:836-841); other passes ignore it.
 __global__ void k_records(const unsigned int* __restrict__ val, const unsigned int* __restrict__ pos,
                           const int* __restrict__ cfi, const unsigned long long* __restrict__ key, long long nvalid,
-                          int mbits, int ncf, long long ntiles, int ntx, int tile, int smax, int Wp, int Wy,
+                          int mbits, int ncf, int kos2, long long ntiles, int ntx, int tile, int smax, int Wp, int Wy,
                           const int* __restrict__ cfsize, int nx, int ny, int4* __restrict__ rec) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
     const unsigned int s = val[i];
@@ -1125,7 +1167,7 @@ __global__ void k_records(const unsigned int* __restrict__ val, const unsigned i
     const int c = cfi[s];
     const int w = cfsize[c];
     const int sup = (w - 1) / 2;
-    const long long t = key_tile(key[i], mbits, ncf) % ntiles;
+    const long long t = key_tile(key[i], mbits, ncf, kos2) % ntiles;
     const int tx = (int)(t % ntx), ty = (int)(t / ntx);
     const int px0 = (int)(ps & 0xffffu) - sup - (tx * tile - smax);
     const int py0 = (int)(ps >> 16) - sup - (ty * tile - smax);
@@ -1137,88 +1179,94 @@ __global__ void k_records(const unsigned int* __restrict__ val, const unsigned i
   }
 }
 
-// Per sorted sample, once per grid pass: rVis = phasor * conj(vis) * wt (* mfs)
-// (TableVisGridder.cc:775-806), or wt (* mfs) for the PSF.
-// Gathers the weighted visibilities of the sorted samples (phase rotation,
-// conjugation, weight and MFS factor of TableVisGridder::generic) and adds the
-// weights into the sums of weights, in double, per (CF row, pol, image channel)
-// (TableVisGridder.cc:783-823).  The records are sorted by tile and CF index,
-// so neighbouring samples mostly share one sum-of-weights row: a segmented
-// warp scan adds each run of equal rows once, one atomic per polarisation,
-// instead of one per sample.
-__global__ void k_gather_vis(VisArgs v, const int4* __restrict__ rec, long long nvalid, float2* __restrict__ out,
-                             SumwArgs sw, DevError* err) {
+// Per sorted sample, once per grid pass: the weight checks and
+// itsSumWeights(row, pol, image channel) += wt in double (TableVisGridder.cc:
+// 783-823) over the sorted records, whose equal sum-of-weights rows come in
+// long runs.  Each warp takes chunks of kSumwChunk consecutive samples, 32 at
+// a time; a segmented warp scan sums each run of equal rows inside the 32, and
+// the run still open at the end of a window is carried into the next window,
+// so a run costs one atomic per polarisation per chunk instead of one per 32
+// samples (many warps adding into the same few rows at once is what bounds
+// this pass).  The sums are exact in FP64 for weights in [1/4, 4], whatever
+// the order of the additions.
+constexpr int kSumwChunk = 1024;
+
+__global__ void k_sum_weights(VisArgs v, const int4* __restrict__ rec, long long nvalid, SumwArgs sw, DevError* err) {
   const long long n = v.nrow * (long long)v.nchan;
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = blockIdx.x * (long long)blockDim.x + threadIdx.x - lane; base < nvalid; base += stride) {
-    const long long i = base + lane;
-    long long bin = -1;
-    float wts[4] = {0.f, 0.f, 0.f, 0.f};
-    if (i < nvalid) {
-      const int4 r = rec[i];
-      const long long s = r.w;
-      const unsigned nr32 = (unsigned)v.nrow;       // plans hold fewer than 2^31 samples
-      const int chan = (int)((unsigned)r.w / nr32);
-      const long long row = (long long)((unsigned)r.w - (unsigned)chan * nr32);
-      float pr = 1.f, pi = 0.f;
-      if (out) phasor_of(v, row, chan, &pr, &pi);
-      const float m = v.mfs ? v.mfs[chan] : 1.f;
-      bool good = true;
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long c0 = warp0 * kSumwChunk; c0 < nvalid; c0 += nwarps * kSumwChunk) {
+    const long long c1 = min(nvalid, c0 + kSumwChunk);
+    long long cbin = -1;                   // the carried run (same in every lane)
+    double cacc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long base = c0; base < c1; base += 32) {
+      const long long i = base + lane;
+      long long bin = -2;                  // past the chunk: a run of its own, never added
+      float wts[4] = {0.f, 0.f, 0.f, 0.f};
+      if (i < c1) {
+        bin = -1;
+        const int4 r = rec[i];
+        const long long smp = r.w;
+        const unsigned nr32 = (unsigned)v.nrow;     // plans hold fewer than 2^31 samples
+        const int chan = (int)((unsigned)r.w / nr32);
+        bool good = true;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          if (p >= v.npol) break;
+          const float wt = noise_weight(v.noise ? v.noise[smp + n * p].x : 1.f);
+          if (!(wt > 0.f)) good = false;
+          wts[p] = wt;
+        }
+        if (!good) raise_error(err, YG_ERR_WEIGHT, smp);
+        if (sw.sumw && good) {
+          const int rr = sw.track_per_os ? r.z : r.z / (sw.os * sw.os);
+          const int ic = sw.chan_map[chan];
+          if (rr < 0 || rr >= sw.nrows || ic < 0 || ic >= sw.nchan_img) {
+            raise_error(err, YG_ERR_CINDEX, smp);
+          } else {
+            bin = rr + (long long)sw.nrows * v.npol * ic;
+          }
+        }
+      }
+      if (!sw.sumw) continue;              // uniform over the grid: no lane leaves the shuffles
+      const long long prev = __shfl_up_sync(full, bin, 1);
+      const unsigned heads = __ballot_sync(full, lane == 0 || prev != bin);
+      const int seg0 = 31 - __clz(heads & (full >> (31 - lane)));
+      const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+      const bool first = seg0 == 0;        // this lane's run starts the window
+      const bool last = lane == 31 || (heads >> (lane + 1)) == 0u;   // no run starts after this lane
+      const long long bin0 = __shfl_sync(full, bin, 0);
+      const bool cont = bin0 == cbin;      // the window's first run continues the carried one
+      // the carried run ends here: add it
+      if (!cont && cbin >= 0 && lane == 0) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+          if (p < v.npol) atomicAdd(&sw.sumw[cbin + (long long)sw.nrows * p], cacc[p]);
+      }
+      double lastsum[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int p = 0; p < 4; ++p) {
         if (p >= v.npol) break;
-        const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
-        const float wt = noise_weight(nre);
-        if (!(wt > 0.f)) good = false;
-        wts[p] = wt;
-        if (!out) continue;   // checks and sums of weights only
-        float2 o;
-        if (v.pcf) {
-          // uVis = wt: the preconditioner ignores the MFS weight
-          o.x = __fmul_rn(1.f, wt);
-          o.y = __fmul_rn(0.f, wt);
-        } else if (v.psf) {
-          o.x = __fmul_rn(__fmul_rn(1.f, wt), m);
-          o.y = __fmul_rn(__fmul_rn(0.f, wt), m);
-        } else {
-          const float2 vv = v.vis[s + n * p];
-          const float vr = vv.x, vi = -vv.y;
-          float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
-          float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
-          rr = __fmul_rn(__fmul_rn(rr, wt), m);
-          ri = __fmul_rn(__fmul_rn(ri, wt), m);
-          o = make_float2(rr, ri);
+        double x = bin >= 0 ? (double)wts[p] : 0.0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const double y = __shfl_up_sync(full, x, off);
+          if (lane - off >= seg0) x += y;
         }
-        out[(size_t)i * v.npol + p] = o;
+        if (first && cont) x += cacc[p];
+        if (tail && !last && bin >= 0) atomicAdd(&sw.sumw[bin + (long long)sw.nrows * p], x);
+        lastsum[p] = __shfl_sync(full, x, 31);
       }
-      if (!good) raise_error(err, YG_ERR_WEIGHT, s);
-      if (sw.sumw && good) {
-        const int rr = sw.track_per_os ? r.z : r.z / (sw.os * sw.os);
-        const int ic = sw.chan_map[chan];
-        if (rr < 0 || rr >= sw.nrows || ic < 0 || ic >= sw.nchan_img) {
-          raise_error(err, YG_ERR_CINDEX, s);
-        } else {
-          bin = rr + (long long)sw.nrows * v.npol * ic;
-        }
-      }
+      cbin = __shfl_sync(full, bin, 31);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) cacc[p] = lastsum[p];
     }
-    if (!sw.sumw) continue;    // uniform over the grid: no lane is left out of the shuffles
-    const long long prev = __shfl_up_sync(full, bin, 1);
-    const unsigned heads = __ballot_sync(full, lane == 0 || prev != bin);
-    const int seg0 = 31 - __clz(heads & (full >> (31 - lane)));
-    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (sw.sumw && cbin >= 0 && lane == 0) {
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      if (p >= v.npol) break;
-      double x = bin >= 0 ? (double)wts[p] : 0.0;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const double y = __shfl_up_sync(full, x, off);
-        if (lane - off >= seg0) x += y;
-      }
-      if (tail && bin >= 0) atomicAdd(&sw.sumw[bin + (long long)sw.nrows * p], x);
+      for (int p = 0; p < 4; ++p)
+        if (p < v.npol) atomicAdd(&sw.sumw[cbin + (long long)sw.nrows * p], cacc[p]);
     }
   }
 }
@@ -1230,12 +1278,12 @@ __global__ void k_inverse(const int4* __restrict__ rec, long long nvalid, int* _
     inv[rec[i].w] = (int)i;
 }
 
-// The weighted visibilities of k_gather_vis (same arithmetic), read in the
-// cube's own order (sample s = row + nrow * chan, one thread per sample, so
-// each polarisation plane is read in coalesced runs) and written to the
+// The weighted visibilities (weighted_vis), read in the cube's own order
+// (sample s = row + nrow * chan, one thread per sample, so each polarisation
+// plane is read in coalesced runs) and written to the
 // sample's sorted slot inv[s] (its npol values are one contiguous 8 npol-byte
-// block).  The weight checks and the sums of weights stay with k_gather_vis
-// over the sorted records, where equal sum-of-weights rows come in runs.
+// block).  The weight checks and the sums of weights are k_sum_weights' over
+// the sorted records, where equal sum-of-weights rows come in runs.
 __global__ void k_gather_cube(VisArgs v, const int* __restrict__ inv, float2* __restrict__ out) {
   const long long n = v.nrow * (long long)v.nchan;
   const unsigned nr32 = (unsigned)v.nrow;       // plans hold fewer than 2^31 samples
@@ -1251,21 +1299,7 @@ __global__ void k_gather_cube(VisArgs v, const int* __restrict__ inv, float2* __
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
       if (p >= v.npol) break;
-      const float nre = v.noise ? v.noise[s + n * p].x : 1.f;
-      const float wt = noise_weight(nre);
-      if (v.pcf) {
-        o[p] = make_float2(__fmul_rn(1.f, wt), __fmul_rn(0.f, wt));
-      } else if (v.psf) {
-        o[p] = make_float2(__fmul_rn(__fmul_rn(1.f, wt), m), __fmul_rn(__fmul_rn(0.f, wt), m));
-      } else {
-        const float2 vv = v.vis[s + n * p];
-        const float vr = vv.x, vi = -vv.y;
-        float rr = __fsub_rn(__fmul_rn(pr, vr), __fmul_rn(pi, vi));
-        float ri = __fadd_rn(__fmul_rn(pr, vi), __fmul_rn(pi, vr));
-        rr = __fmul_rn(__fmul_rn(rr, wt), m);
-        ri = __fmul_rn(__fmul_rn(ri, wt), m);
-        o[p] = make_float2(rr, ri);
-      }
+      o[p] = weighted_vis(v, s, n, p, pr, pi, m);
     }
     float2* dst = out + (size_t)i * v.npol;
     if (v.npol == 4) {
@@ -1279,23 +1313,6 @@ __global__ void k_gather_cube(VisArgs v, const int* __restrict__ inv, float2* __
         if (p < v.npol) dst[p] = o[p];
     }
   }
-}
-
-// Run ends of the sorted list (a run = consecutive samples of one tile with
-// the same CF index).  rev[j], j = nvalid-1-i, holds i+1 when a new run starts
-// at i+1 (or i+1 == nvalid) and INT_MAX otherwise; a prefix-min over rev gives
-// for every i the first run start after it.
-__global__ void k_run_marks(const unsigned long long* __restrict__ key, long long nvalid, int mbits,
-                            int* __restrict__ rev) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x) {
-    const bool brk = (i + 1 == nvalid) || ((key[i + 1] >> mbits) != (key[i] >> mbits));
-    rev[nvalid - 1 - i] = brk ? (int)(i + 1) : 0x7fffffff;
-  }
-}
-
-__global__ void k_run_unreverse(const int* __restrict__ revmin, long long nvalid, int* __restrict__ runend) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid; i += (long long)gridDim.x * blockDim.x)
-    runend[i] = revmin[nvalid - 1 - i];
 }
 
 // ---------------------------------------------------------------------------
@@ -2160,7 +2177,8 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   YG_CUDA_TRY(cudaMemsetAsync(pl.tstart.p, 0, nt * 4, st));
   YG_CUDA_TRY(cudaMemsetAsync(pl.tend.p, 0, nt * 4, st));
   YG_CUDA_TRY(cudaMemsetAsync(pl.nvalid_d.p, 0, 16, st));
-  k_tile_bounds<<<grid_dim(n, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), n, a.mbits, a.cf.ncf,
+  const int kos2 = a.key_planes ? a.os * a.os : 1;
+  k_tile_bounds<<<grid_dim(n, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), n, a.mbits, a.cf.ncf, kos2,
                                                   a.invalid_key, pl.tstart.as<int>(), pl.tend.as<int>(),
                                                   pl.nvalid_d.as<long long>());
   YG_COUNT_LAUNCH();
@@ -2181,36 +2199,38 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
   k_fill_items<<<grid_dim(nt, 256), 256, 0, st>>>(pl.tstart.as<int>(), pl.tend.as<int>(), pl.nit.as<int>(),
                                                   pl.itembase.as<int>(), nt, vmax, pl.items.as<int4>());
   YG_COUNT_LAUNCH();
-  YG_CUDA_TRY(pl.runend.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * 4));
-  if (pl.nvalid > 0) {
-    // scratch for the marks: the (now unused) alternate key buffer
-    int* rev = pl.key_alt.as<int>();
-    int* revmin = rev + pl.nvalid;
-    k_run_marks<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.key.as<unsigned long long>(), pl.nvalid, a.mbits, rev);
-    YG_COUNT_LAUNCH();
-    if (scan_tmp_bytes(pl.nvalid) > pl.sort_tmp.bytes) YG_CUDA_TRY(pl.sort_tmp.ensure(scan_tmp_bytes(pl.nvalid)));
-    YG_CUDA_TRY(scan_i32(rev, revmin, pl.nvalid, SCAN_MIN, false, pl.sort_tmp.p, pl.sort_tmp.bytes, st));
-    k_run_unreverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(revmin, pl.nvalid, pl.runend.as<int>());
-    YG_COUNT_LAUNCH();
-  }
   YG_CUDA_TRY(pl.rec.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * sizeof(int4)));
   if (pl.nvalid > 0) {
     if (a.cf.wpad > 1023 || !a.cf.pad) return YG_ERR_UNSUPPORTED;  // residues are packed in 10 bits
     k_records<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.val.as<unsigned int>(), pl.pos.as<unsigned int>(),
                                                         pl.cfi.as<int>(), pl.key.as<unsigned long long>(), pl.nvalid,
-                                                        a.mbits, a.cf.ncf, (long long)a.ntx * a.nty, a.ntx, a.tile,
+                                                        a.mbits, a.cf.ncf, kos2, (long long)a.ntx * a.nty, a.ntx, a.tile,
                                                         pl.smax, a.cf.wpad, pl.wy, a.cf.size, a.nx, a.ny,
                                                         pl.rec.as<int4>());
     YG_COUNT_LAUNCH();
   }
-  YG_CUDA_TRY(pl.inv.ensure((size_t)n * 4));
-  YG_CUDA_TRY(cudaMemsetAsync(pl.inv.p, 0xff, (size_t)n * 4, st));
-  if (pl.nvalid > 0) {
-    k_inverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.rec.as<int4>(), pl.nvalid, pl.inv.as<int>());
-    YG_COUNT_LAUNCH();
+  pl.inv_ready = pl.inv_pos_ready = false;
+  if (a.need_inv && !a.key_planes) {
+    YG_CUDA_TRY(pl.inv.ensure((size_t)n * 4));
+    YG_CUDA_TRY(cudaMemsetAsync(pl.inv.p, 0xff, (size_t)n * 4, st));
+    if (pl.nvalid > 0) {
+      k_inverse<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(pl.rec.as<int4>(), pl.nvalid, pl.inv.as<int>());
+      YG_COUNT_LAUNCH();
+    }
+    pl.inv_ready = true;
   }
   pl.pos_ready = false;
-  if (a.pos_major && pl.nvalid > 0) {
+  pl.grid_only = false;
+  if (a.key_planes) {
+    // a gridding-only plan sorted once by the plane-major key: its records
+    // are the plane-major order itself (no CF-major records, no second sort)
+    std::swap(pl.rec.p, pl.rec_pos.p);
+    std::swap(pl.rec.bytes, pl.rec_pos.bytes);
+    pl.grid_only = true;
+    pl.pos_ready = pl.nvalid > 0;
+    pl.pos_mode = 2;
+    pl.os2 = a.os * a.os;
+  } else if (a.pos_major && pl.nvalid > 0) {
     // a second order of the same records for gridding: tile first as before
     // (the work items stay valid), then the position inside the tile, then
     // the CF index, so consecutive samples of an item mostly cover the same
@@ -2235,10 +2255,14 @@ int plan_build(Plan& pl, const BinArgs& a, int vmax, DevError* err, cudaStream_t
                                                      alt2 ? pl.pos_val2.as<unsigned int>() : pl.val_alt.as<unsigned int>(),
                                                      nv, pl.rec_pos.as<int4>());
     YG_COUNT_LAUNCH();
-    YG_CUDA_TRY(pl.inv_pos.ensure((size_t)n * 4));
-    YG_CUDA_TRY(cudaMemsetAsync(pl.inv_pos.p, 0xff, (size_t)n * 4, st));
-    k_inverse<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec_pos.as<int4>(), nv, pl.inv_pos.as<int>());
-    YG_COUNT_LAUNCH();
+    if (a.pos_major == 1) {
+      // the position-major kernel reads gathered visibilities in this order
+      YG_CUDA_TRY(pl.inv_pos.ensure((size_t)n * 4));
+      YG_CUDA_TRY(cudaMemsetAsync(pl.inv_pos.p, 0xff, (size_t)n * 4, st));
+      k_inverse<<<grid_dim(nv, 256), 256, 0, st>>>(pl.rec_pos.as<int4>(), nv, pl.inv_pos.as<int>());
+      YG_COUNT_LAUNCH();
+      pl.inv_pos_ready = true;
+    }
     YG_CUDA_TRY(cudaGetLastError());
     pl.pos_ready = true;
     pl.pos_mode = a.pos_major;
@@ -2503,6 +2527,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
                       pl.wy > 0 && pl.wy <= 16 && !cf.varsup && v.npol <= 4;
   const bool pos = !planes && (mode & 32) != 0 && pl.pos_ready && pl.pos_mode == 1 && !learned && v.npol <= 4;
   const bool racc = (mode & 16) != 0 || pos;
+  if (pl.grid_only && !planes && pl.nitems > 0) return YG_ERR_STATE;   // only the plane-major kernel reads it
   // mode 128 (with 64): the plane-major kernel's tile in the item's scratch slot
   const bool gtile = planes && (mode & 128) != 0;
   mode &= 15;
@@ -2526,18 +2551,19 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   const size_t per_item = gtile ? (size_t)v.npol * ((size_t)Pg * Pg + gtile_nthr) * sizeof(float2)
                                 : (size_t)v.npol * P * P * sizeof(float2);
   YG_CUDA_TRY(scratch.ensure_headroom(per_item * pl.nitems));
-  YG_CUDA_TRY(svis.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
   if (v.npol > 4) return YG_ERR_UNSUPPORTED;
   // the weighted visibilities in the order of the records the kernel reads,
-  // gathered in the cube's order; the weight checks and the sums of weights
-  // over the sorted records (CF-major or plane-major: runs of equal
-  // sum-of-weights rows keep the atomics few)
-  k_gather_cube<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, (pos || planes) ? pl.inv_pos.as<int>()
-                                                                               : pl.inv.as<int>(),
-                                                           svis.as<float2>());
-  YG_COUNT_LAUNCH();
-  k_gather_vis<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, planes ? pl.rec_pos.as<int4>() : pl.rec.as<int4>(),
-                                                         pl.nvalid, nullptr, sw, err);
+  // gathered in the cube's order (the plane-major kernel's producer forms its
+  // own); the weight checks and the sums of weights over the sorted records
+  if (!planes) {
+    if (!(pos ? pl.inv_pos_ready : pl.inv_ready)) return YG_ERR_STATE;   // a plan made for degridding only
+    YG_CUDA_TRY(svis.ensure_headroom((size_t)std::max(1ll, pl.nvalid) * v.npol * sizeof(float2)));
+    k_gather_cube<<<grid_dim(pl.nsamples, 256), 256, 0, st>>>(v, pos ? pl.inv_pos.as<int>() : pl.inv.as<int>(),
+                                                             svis.as<float2>());
+    YG_COUNT_LAUNCH();
+  }
+  k_sum_weights<<<grid_dim(pl.nvalid, 256), 256, 0, st>>>(v, planes ? pl.rec_pos.as<int4>() : pl.rec.as<int4>(),
+                                                          pl.nvalid, sw, err);
   YG_COUNT_LAUNCH();
   GridKArgs g;
   g.Wy = pl.wy;
@@ -2545,8 +2571,7 @@ int plan_grid(const Plan& pl, const VisArgs& v, const CFView& cf, float2* grid, 
   g.items = pl.items.as<int4>();
   g.val = pl.val.as<unsigned int>();
   g.rec = pos ? pl.rec_pos.as<int4>() : pl.rec.as<int4>();
-  g.svis = svis.as<float2>();
-  g.runend = pl.runend.as<int>();
+  g.svis = planes ? nullptr : svis.as<float2>();
   g.pos = pl.pos.as<unsigned int>();
   g.cfi = pl.cfi.as<int>();
   g.v = v;
@@ -2717,6 +2742,7 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
                 cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const LearnedCF* lcf, int variant, bool alone) {
   const long long n = pl.nsamples;
   if (n == 0) return YG_OK;
+  if (pl.grid_only) return YG_ERR_STATE;     // no CF-major records
   YG_CUDA_TRY(tmp_vals.ensure((size_t)n * v.npol * sizeof(float2)));
   bool done = false;
   const bool learned = lcf && lcf->w16;

@@ -119,6 +119,8 @@ struct BinArgs {
   int mbits;               // bits of the within-tile Morton code
   int wy;                  // row modulus of the residues in the records (0: the padded CF width)
   int pos_major;           // also build second-order records (rec_pos): 1 position-major, 2 plane-major
+  int key_planes;          // a plan for gridding only: sort once, by the plane-major key (pos_major 2)
+  int need_inv;            // build the inverse permutation (the cube-order gather of the CF-major kernels)
   unsigned long long invalid_key;  // one past the largest valid key
   CFView cf;
 };
@@ -143,12 +145,13 @@ struct Plan {
   bool prev_ready = false;      // order_prev holds this plan's predecessors
   DevBuf last;                  // grid carry: loop-order index of the last used sample
   DevBuf chanmap;               // accessor channel -> image channel of the binned chunk
-  DevBuf runend;                // end of the run of equal (tile, CF) samples containing each sorted index
   DevBuf rec;                   // per sorted sample: cell, residues|w, CF index, sample id (int4)
   DevBuf rec_pos;               // the same records ordered by tile, then position in the tile, then CF
   DevBuf pos_val2;              // alternate values of the rec_pos sort
   DevBuf inv, inv_pos;          // per sample id: its index in rec (rec_pos), -1 off the grid
   bool pos_ready = false;       // rec_pos is built
+  bool grid_only = false;       // sorted once, plane-major: rec_pos only (no CF-major records)
+  bool inv_ready = false, inv_pos_ready = false;   // inv / inv_pos are built
   int pos_mode = 0;             // its order: 1 position then CF index; 2 CF plane, position, offset
   int os2 = 1;                  // oversampling offsets per CF plane
   DevBuf ext;                   // continuous learned CF: per sorted sample (ru, rv, w, 0)
