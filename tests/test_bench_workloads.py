@@ -41,3 +41,17 @@ def test_defaults_keep_the_timing_contract(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse()
     assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1 and a.config == 1 and a.impl == "b200"
+
+
+def test_kernel_names_and_traffic_rates():
+    """The bench line names the kernels a variant runs and scales the grid
+    kernel's captured DRAM rates (None for a kernel with no capture)."""
+    import bench
+    assert bench.kernel_names(193, 6) == ("k_grid_pl", "k_degrid_r")
+    assert bench.kernel_names(0, 6) == ("k_grid", "k_degrid_r")
+    assert bench.kernel_names(193 | 256, 6) == ("k_grid_pl", "k_degrid_t")
+    assert bench.kernel_names(1, 20) == ("k_grid", "k_degrid_t")
+    info = {"tile": 32, "nvalid": 1000, "nitems": 10}
+    per_sample, per_cell = bench.TRAFFIC_RATES["k_grid_pl"]
+    assert bench.kgrid_traffic(info, 6, 4, "k_grid_pl") == int(per_sample * 1000 + per_cell * 10 * 4 * 44 * 44)
+    assert bench.kgrid_traffic(info, 6, 4, "k_grid_unknown") is None

@@ -50,8 +50,7 @@ CycleBatch::~CycleBatch() {
 void CycleBatch::enqueue(Instance& in, cudaStream_t st) {
   const size_t bytes = (size_t)in.obs.nrow * in.obs.nchan * in.obs.npol * sizeof(float2);
   ck(cudaMemsetAsync(in.model_vis.p, 0, bytes, st), "clear model visibilities");
-  // instances run side by side: the degrid kernels' all-warps ring protocol
-  if (!in.dg->is_model_empty()) in.dg->degrid_enqueue(in.model, in.plan, in.mfs_dg, st, nullptr, nullptr, false);
+  if (!in.dg->is_model_empty()) in.dg->degrid_enqueue(in.model, in.plan, in.mfs_dg, st);
   const long long n = (long long)in.obs.nrow * in.obs.nchan * in.obs.npol;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
   k_subtract<<<std::max(1, blocks), 256, 0, st>>>(in.obs.vis, in.model_vis.as<float2>(), in.resid_vis.as<float2>(), n);

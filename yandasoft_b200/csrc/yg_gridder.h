@@ -139,8 +139,8 @@ class Gridder {
   // no allocation once sized, any stream (what a CUDA graph records)
   void grid_enqueue(const Chunk& dc, const Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
                     cudaEvent_t k1 = nullptr);
-  // alone = false where other instances' passes share the GPU (the major-cycle
-  // graph): the degrid kernels then use their all-warps ring protocol
+  // alone = false asks the degrid kernels for their all-warps ring protocol
+  // instead of owned segments
   void degrid_enqueue(Chunk& dc, Plan& pl, const float* mfs, cudaStream_t st, cudaEvent_t k0 = nullptr,
                       cudaEvent_t k1 = nullptr, bool alone = true);
   const float* mfs_weights(const Chunk& dc);

@@ -2786,10 +2786,20 @@ int plan_degrid(Plan& pl, const VisArgs& v, float2* vis_out, const CFView& cf, c
       smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
     }
     d.stage_bytes = seg_stage_bytes(d.cfbuf, xv);
-    // owned segments (the faster protocol) where this pass is the only ring
-    // kernel running; the all-warps protocol where instances share the GPU
-    // (owned segments timed out there)
-    d.own = (alone && d.nstages >= kDegridThreads / 32) ? 1 : 0;
+    // Owned segments need a ring depth that is a multiple of the tap warps:
+    // segment s sits in stage s mod NST and belongs to warp s mod ncw, so then
+    // every stage has one owner, which waits for the stage's fills in order.
+    // With another depth, stage st also holds segments of other warps, and a
+    // warp could begin waiting for the stage's next fill while the previous
+    // one (another warp's, its bulk copy still in flight) had not completed:
+    // the parity wait takes the incomplete phase for the one before it and
+    // returns at once, and the warp reads the other segment.
+    const int ncw_d = kDegridThreads / 32;
+    d.own = (alone && d.nstages >= ncw_d) ? 1 : 0;
+    if (d.own && !learned) {   // (the learned forms' rings hold at most ncw stages)
+      d.nstages = d.nstages / ncw_d * ncw_d;
+      smem = degrid_t_smem_bytes(v.npol, d.Pg, d.cfbuf, d.nstages);
+    }
     if (d.nstages > 0) {
       if (ev0) cudaEventRecord(ev0, st);
       const int threads = kDegridThreads + 32;   // tap warps + the producer warp
