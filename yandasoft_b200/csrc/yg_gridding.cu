@@ -5,21 +5,31 @@
 //                  oversample offsets, w-plane, CF index, strict on-grid test
 //                  (TableVisGridder.cc:604-764), and a 64-bit sort key
 //                  (grid plane, image channel, uv tile, CF index, Morton
-//                  position inside the tile).
+//                  position inside the tile; or, for a gridding-only plan of
+//                  the plane-major kernel, tile, CF plane, position, offset).
 //   radix sort     stable LSD radix sort of (key, sample id) (yg_sort.cu).
 //   k_tile_bounds  start/end of every tile's run in the sorted list.
 //   work items     tiles split into items of at most vmax samples.
-//   k_grid         one CTA per item: the padded tile (T + 2 Smax)^2 lives in
-//                  shared memory; every thread owns the cells of a fixed
-//                  residue class (x mod W, y mod W), W = 2 Smax + 1, so no two
-//                  threads ever touch the same cell and the tap sums run in
-//                  registers until a thread's cell changes (no atomics).  The
-//                  padded tile is flushed once to a per-item scratch slot.
+//   k_records      one 16-byte record per sorted sample (footprint origin,
+//                  residues, CF width and index, sample id).
+//   k_sum_weights  weight checks and sums of weights over the sorted records.
+//   k_grid         one CTA per item over CF-major records: the padded tile
+//                  (T + 2 Smax)^2 lives in shared memory; every thread owns
+//                  the cells of a fixed residue class (x mod W, y mod W), so no
+//                  two threads ever touch the same cell (no atomics); its
+//                  weighted visibilities come from k_gather_cube.
+//   k_grid_pl      the same over plane-major records, each CF plane's
+//                  oversampling offsets staged in shared memory once, running
+//                  sums in registers, the tile in shared or global memory; its
+//                  producer warp forms the weighted visibilities itself.
 //   k_halo_sum     each output tile adds, in a fixed order, the overlapping
-//                  parts of its neighbours' padded tiles: deterministic, no
-//                  atomics, and the grid is written once.
-//   k_degrid       one CTA per item: the padded grid tile is staged in shared
-//                  memory, one warp per visibility, warp-shuffle reduction.
+//                  parts of its neighbours' padded tiles: deterministic, and
+//                  the grid is written once.
+//   k_degrid_r     16-wide CFs: one CTA per item, the padded grid tile in
+//                  shared memory, a warp per segment with its CF column in
+//                  registers, two samples per half-warp pass.
+//   k_degrid_t     wider CFs (and the learned forms): the CF plane per tap
+//                  from the ring, transposing warp-shuffle reductions.
 //   k_degrid_writeback  the reference's write-back semantics, including the
 //                  value it carries into off-grid samples.
 #include <algorithm>
