@@ -1462,20 +1462,50 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
   const int nwarps = blockDim.x >> 5;
   const float2* src = a.smem_grid ? g_s : gbase;
   const long long pstride = a.smem_grid ? P2 : plane_cells;
-  for (int i = it.y + warp; i < it.z; i += nwarps) {
-    const int4 r = a.rec[i];
+  // One sample: the taps of its CF (the reference's loop), then the warp sum
+  // and the write-out.  The records are in CF order, so two consecutive
+  // samples often share their CF: a warp then takes both at once and each CF
+  // tap and offset is loaded once for the two (the same sums in the same order).
+  auto finish = [&](const int4 r, float (&re)[4][NPOL], float (&im)[4][NPOL]) {
     const unsigned int s = (unsigned int)r.w;
-    const int c = r.z;
-    const int w = (r.y >> 20) & 1023;
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) {
+      float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
+      float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+      }
+      re[0][p] = sr;
+      im[0][p] = si;
+    }
+    if (lane == 0) {
+      const long long row = s % a.v.nrow;
+      const int chan = (int)(s / a.v.nrow);
+      float pr, pi;
+      phasor_of(a.v, row, chan, &pr, &pi);
+      const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        float cr = re[0][p], ci = im[0][p];
+        if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
+        const float orr = __fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi));
+        const float oi = __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr));
+        a.out[(size_t)s * NPOL + p] = make_float2(orr, oi);
+      }
+    }
+  };
+  // the footprint origin of a record in the grid source (tile or grid)
+  auto origin_of = [&](const int4 r) -> long long {
     const int px0 = r.x & 0xffff, py0 = (r.x >> 16) & 0xffff;
-    const long long origin = a.smem_grid ? (long long)px0 + (long long)P * py0
-                                         : (long long)(X0 + px0) + (long long)a.nx * (Y0 + py0);
-    const float2* __restrict__ cfp = a.cf.data + a.cf.off[c];
-    float re[4][NPOL], im[4][NPOL];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) { re[u][p] = 0.f; im[u][p] = 0.f; }
+    return a.smem_grid ? (long long)px0 + (long long)P * py0
+                       : (long long)(X0 + px0) + (long long)a.nx * (Y0 + py0);
+  };
+  auto taps_one = [&](const int4 r, float (&re)[4][NPOL], float (&im)[4][NPOL]) {
+    const int w = (r.y >> 20) & 1023;
+    const long long origin = origin_of(r);
+    const float2* __restrict__ cfp = a.cf.data + a.cf.off[r.z];
     const int ntaps = w * w;
     if (w == W) {
       for (int tp = lane; tp < ntaps; tp += 128) {
@@ -1510,31 +1540,58 @@ __global__ void __launch_bounds__(kDegridThreads) k_degrid(DegridKArgs a) {
         }
       }
     }
+  };
+  auto zero = [&](float (&re)[4][NPOL], float (&im)[4][NPOL]) {
 #pragma unroll
-    for (int p = 0; p < NPOL; ++p) {
-      float sr = (re[0][p] + re[1][p]) + (re[2][p] + re[3][p]);
-      float si = (im[0][p] + im[1][p]) + (im[2][p] + im[3][p]);
+    for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, off);
-        si += __shfl_xor_sync(0xffffffffu, si, off);
+      for (int p = 0; p < NPOL; ++p) { re[u][p] = 0.f; im[u][p] = 0.f; }
+  };
+  // (pairs for up to two polarisations: four would double 32 accumulators)
+  constexpr bool PAIR = NPOL <= 2;
+  for (int i = it.y + 2 * warp; i < it.z; i += 2 * nwarps) {
+    const int4 r0 = a.rec[i];
+    const bool has1 = i + 1 < it.z;
+    const int4 r1 = has1 ? a.rec[i + 1] : r0;
+    float re[4][NPOL], im[4][NPOL];
+    zero(re, im);
+    if (PAIR && has1 && r1.z == r0.z && ((r0.y >> 20) & 1023) == W) {
+      float re1[4][NPOL], im1[4][NPOL];
+      zero(re1, im1);
+      const float2* __restrict__ cfp = a.cf.data + a.cf.off[r0.z];
+      const long long o0 = origin_of(r0), o1 = origin_of(r1);
+      const int ntaps = W2;
+      for (int tp = lane; tp < ntaps; tp += 128) {
+        int o[4];
+        float2 cv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int tu = tp + 32 * u;
+          o[u] = tu < ntaps ? tab[tu] : 0;
+          cv[u] = tu < ntaps ? __ldg(cfp + tu) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            const float2 g = src[pstride * p + o0 + o[u]];
+            const float2 h = src[pstride * p + o1 + o[u]];
+            re[u][p] = fmaf(cv[u].x, g.x, fmaf(cv[u].y, g.y, re[u][p]));
+            im[u][p] = fmaf(cv[u].y, g.x, fmaf(-cv[u].x, g.y, im[u][p]));
+            re1[u][p] = fmaf(cv[u].x, h.x, fmaf(cv[u].y, h.y, re1[u][p]));
+            im1[u][p] = fmaf(cv[u].y, h.x, fmaf(-cv[u].x, h.y, im1[u][p]));
+          }
+        }
       }
-      re[0][p] = sr;
-      im[0][p] = si;
-    }
-    if (lane == 0) {
-      const long long row = s % a.v.nrow;
-      const int chan = (int)(s / a.v.nrow);
-      float pr, pi;
-      phasor_of(a.v, row, chan, &pr, &pi);
-      const float m = a.v.mfs ? a.v.mfs[chan] : 1.f;
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        float cr = re[0][p], ci = im[0][p];
-        if (a.v.mfs) { cr = __fmul_rn(cr, m); ci = __fmul_rn(ci, m); }
-        const float orr = __fsub_rn(__fmul_rn(cr, pr), __fmul_rn(ci, pi));
-        const float oi = __fadd_rn(__fmul_rn(cr, pi), __fmul_rn(ci, pr));
-        a.out[(size_t)s * NPOL + p] = make_float2(orr, oi);
+      finish(r0, re, im);
+      finish(r1, re1, im1);
+    } else {
+      taps_one(r0, re, im);
+      finish(r0, re, im);
+      if (has1) {
+        zero(re, im);
+        taps_one(r1, re, im);
+        finish(r1, re, im);
       }
     }
   }
