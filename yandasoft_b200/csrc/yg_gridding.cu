@@ -1642,7 +1642,7 @@ struct DegridTArgs {
   long long ntiles;
   int smax, Pg, Wp, cfbuf;
   int stage_bytes, nstages;
-  int own;                   // segments owned by one warp each (needs nstages >= tap warps)
+  int own;                   // segments owned by one warp each (nstages a multiple of the tap warps)
   LearnedCF lcf;             // the network of the learned CF mode
   const float4* ext;         // continuous learned CF: per sorted sample (ru, rv, w, 0)
   float2* out;
